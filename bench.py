@@ -1,0 +1,286 @@
+#!/usr/bin/env python
+"""Benchmark of the plain FP64 HPR iteration on the large sparse SOCP
+(n = 2,000,000, m = 1,500,000, nnz(A) = 25M, 20 x 5000 / 5k x 50 / 100k x 3
+variable cones, 100k x 3 + 4k x 50 constraint cones; seeded synthetic data).
+
+A step is one HPR iteration (x half-step over A' and y half-step over A, both
+fused SpMV + projection + Halpern kernels).  `value` is iterations/s with all
+data resident in HBM (A and A' are ~600 MB, far larger than the 126 MB L2, so
+no flush is needed between steps); `e2e` is the same metric through the public
+C ABI from host buffers: upload, scaling, eigenvalue estimate, K iterations
+and the solution read-back all inside the timed region.
+
+--impl reference times the CPU restatement of the reference solver (the
+oracle, the only CPU implementation of this path that runs here) with every
+host thread, on the same instance and metric.
+
+Multi-GPU: the path does not shard (one solve per GPU); --gpus N runs N
+independent replicas, one per rank, and reports the aggregate rate.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hpr-socp_b200"))
+
+WORKLOAD = ("sparse SOCP n=2,000,000 m=1,500,000 nnz(A)=25M (A1 1M lognormal rows, A2 0.5M rows), "
+            "var cones 100k x3 + 5k x50 + 20 x5000, con cones 100k x3 + 4k x50, Q=0")
+METRIC = "HPR iters/s"
+
+
+def measured_peak():
+    for p in (os.path.join(ROOT, "MEASURED_PEAKS.json"), "/root/repo/MEASURED_PEAKS.json"):
+        try:
+            with open(p) as f:
+                d = json.load(f)
+            return float(d["hbm_gbs"]), "measured"
+        except (OSError, KeyError, ValueError):
+            continue
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device=0):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = max(smax, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init(n_gpus):
+    if n_gpus <= 1 or "RANK" not in os.environ:
+        return 0, 1, None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    rank, world = int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"])
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, world, dist
+
+
+def dist_max(dist, v):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_iteration_rate(model, iters=3, threads=0):
+    """Oracle (CPU restatement) iterations/s on this host's cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle_ctx import OracleContext
+    from hprsocp_b200 import HPRSOCP_parameters
+    o = OracleContext(model, threads=threads)
+    o.scale(HPRSOCP_parameters(verbose=False))
+    o.set_sigma_lambda(1.0, 1.05 * 4000.0, 0.0)
+    o.iterate(1, False)
+    t = time.perf_counter()
+    o.iterate(iters, True)
+    dt = time.perf_counter() - t
+    o.close()
+    return iters / dt
+
+
+def run_reference(args, model):
+    cores = os.cpu_count() or 1
+    rate_steps = []
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle_ctx import OracleContext
+    from hprsocp_b200 import HPRSOCP_parameters
+    o = OracleContext(model, threads=0)
+    o.scale(HPRSOCP_parameters(verbose=False))
+    o.set_sigma_lambda(1.0, 1.05 * 4000.0, 0.0)
+    for _ in range(args.warmup):
+        o.iterate(1, False)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        o.iterate(1, k == args.steps - 1)
+    dt = time.perf_counter() - t0
+    o.close()
+    v = args.steps / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "iter/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, seed 1)",
+            "config": {"workload": WORKLOAD, "path": "CPU restatement of the reference iteration (oracle port)"},
+            "cpu_baseline": {"value": v, "unit": "iter/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} HPR iterations of the benchmark instance"},
+            "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="shrink the instance (testing only)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    from hprsocp_b200 import instances
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return
+        model = instances.config1(1, scale=args.scale)
+        run_reference(args, model)
+        return
+
+    rank, world, dist = dist_init(args.gpus)
+    import ctypes as C
+    from hprsocp_b200 import Context, HPRSOCP_parameters, _abi
+    model = instances.config1(1, scale=args.scale)
+    dev = int(os.environ.get("LOCAL_RANK", "0")) if dist is not None else 0
+
+    # ---- device-resident iterations
+    ctx = Context(model, device=dev)
+    info = ctx.scale(HPRSOCP_parameters(verbose=False))
+    lam = ctx.power_A() * 1.05
+    sigma = info["norm_b"] / info["norm_c"]
+    ctx.set_sigma_lambda(sigma, lam, 0.0)
+    ctx.set_inner(0)
+    ctx.iterate(args.warmup, False)
+    barrier(dist)
+    with ClockSampler(dev) as clk:
+        ctx.iterate(args.steps, True)  # device-timed with CUDA events inside
+    ms, launches = ctx.last_iterate()
+    ms = dist_max(dist, ms)
+    bytes_iter = ctx.iteration_bytes()
+    ctx.close()
+    value = world * args.steps / (ms / 1e3)
+    per_iter_ms = ms / args.steps
+    peak, peak_kind = measured_peak()
+    achieved = bytes_iter / (per_iter_ms / 1e3) / 1e9
+
+    # ---- end to end through the C ABI from host buffers
+    e2e = None
+    if not args.no_e2e:
+        lib = _abi.load_library()
+        prob = model.to_c()
+        p = HPRSOCP_parameters(verbose=False, max_iter=args.steps, stoptol=0.0, check_iter=150,
+                               print_frequency=10**9).to_c()
+        m, n = model.m, model.n
+        import numpy as np
+        x, y, z = np.zeros(n), np.zeros(m), np.zeros(n)
+        r = _abi.hpr_results()
+        r.x, r.y, r.z = _abi.dptr(x), _abi.dptr(y), _abi.dptr(z)
+        barrier(dist)
+        t0 = time.perf_counter()
+        rc = lib.hpr_optimize(C.byref(prob), C.byref(p), C.byref(r))
+        dt = time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError(f"hpr_optimize failed: {rc}")
+        dt = dist_max(dist, dt)
+        e2e = {"value": world * r.iter / dt, "unit": "iter/s", "h2d_bytes_per_step": model.nbytes(),
+               "d2h_bytes_per_step": int(x.nbytes + y.nbytes + z.nbytes),
+               "what": "hpr_optimize from host arrays: upload + scaling + power iteration + "
+                       f"{r.iter} iterations (checks every 150) + unscaled solution read-back",
+               "seconds": dt}
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if not args.no_cpu:
+        iters = 3
+        cpu_rate = cpu_iteration_rate(model, iters=iters, threads=0)
+        cpu = {"value": cpu_rate, "unit": "iter/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{iters} HPR iterations of the benchmark instance on the oracle (all host threads)"}
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "engine_config1_dram_bytes.txt")
+    if os.path.exists(tfile):
+        try:
+            traffic = float(open(tfile).read().split()[0])
+        except (ValueError, IndexError):
+            traffic = None
+    line = {
+        "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_iter_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, seed 1)",
+        "config": {"workload": WORKLOAD, "precision": "fp64", "l2": "inputs larger than L2 (A + A' ~ 600 MB)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "scale": args.scale},
+        "hbm_gbs": achieved,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_iter": bytes_iter,
+                     "kernel": "engine_kernel (x half-step over A' + y half-step over A, per iteration)"},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1009 @@
+// hpr_api.cu — the C ABI (include/hprsocp_b200.h): context, upload with
+// validation, workspace, vector access and the solve loop.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+
+#include "hpr_engine.cuh"
+
+namespace hpr {
+
+int set_err(Ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int dev_alloc(Ctx* c, void** p, size_t bytes) {
+  bytes = (bytes + 255) & ~(size_t)255;
+  if (c->used + bytes > c->budget)
+    return set_err(c, HPR_E_BUDGET,
+                   "HBM budget exceeded: need " + std::to_string(c->used + bytes) + " of " + std::to_string(c->budget));
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) return set_err(c, HPR_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  c->used += bytes;
+  return HPR_OK;
+}
+
+namespace {
+
+using std::vector;
+
+void free_all(Ctx* c) {
+  auto f = [](void* p) {
+    if (p) cudaFree(p);
+  };
+  for (DevCSR* M : {&c->A, &c->AT, &c->Q, &c->F, &c->FT}) {
+    f(M->rowptr);
+    f(M->col);
+    f(M->val);
+    f(M->val32);
+    f(M->val16);
+    *M = DevCSR();
+  }
+  for (Plan* p : {&c->planX, &c->planY, &c->planQ, &c->planF}) {
+    f(p->d_tasks);
+    f(p->d_big);
+    f(p->d_lng);
+    f(p->d_big_cnt);
+    f(p->d_lng_cnt);
+    f(p->d_partials);
+    f(p->d_raw);
+    *p = Plan();
+  }
+  double** vs[] = {&c->c,      &c->l,      &c->u,      &c->AL,       &c->AU,     &c->soc_rhs, &c->soc_rhs_full,
+                   &c->qdiag,  &c->row_norm, &c->col_norm, &c->diag_Q, &c->fact1, &c->fact2,   &c->fact,
+                   &c->fact_M, &c->x,      &c->x_hat,  &c->x_bar,    &c->last_x, &c->z_bar,   &c->dx,
+                   &c->y,      &c->y_bar,  &c->last_y, &c->s,        &c->dy,     &c->w,       &c->w_bar,
+                   &c->last_w, &c->dw,     &c->Qw,     &c->dQw,      &c->Qx,     &c->tempv,   &c->ATy,
+                   &c->ATy_bar, &c->last_ATy, &c->ATdy, &c->QATdy,   &c->Rp,     &c->Rd,      &c->Ax,
+                   &c->ftmp,   &c->ftmp2,  &c->vtmp_n, &c->vtmp_m,   &c->pz,     &c->pq,      &c->ptq,
+                   &c->d_red,  &c->d_red_out};
+  for (double** v : vs) {
+    f(*v);
+    *v = nullptr;
+  }
+  f(c->g32_n);
+  f(c->g32_m);
+  c->g32_n = c->g32_m = nullptr;
+  f(c->d_con_start);
+  f(c->d_var_start);
+  c->d_con_start = c->d_var_start = nullptr;
+  f(c->d_state);
+  c->d_state = nullptr;
+  if (c->graph_partial) cudaGraphExecDestroy(c->graph_partial);
+  c->graph_partial = nullptr;
+  c->graph_iters = 0;
+  c->red_slots = 0;
+  c->used = 0;
+  c->uploaded = c->scaled = false;
+}
+
+bool finite_all(const double* v, int64_t n) {
+  for (int64_t i = 0; i < n; ++i)
+    if (!std::isfinite(v[i])) return false;
+  return true;
+}
+bool nonan_all(const double* v, int64_t n) {
+  for (int64_t i = 0; i < n; ++i)
+    if (std::isnan(v[i])) return false;
+  return true;
+}
+
+// Validated 0-based host copy of a CSR matrix with sorted rows.
+int load_csr(Ctx* c, const hpr_csr& s, int base, int64_t nr, int64_t nc, const char* name, vector<int32_t>& rp,
+             vector<int32_t>& ci, vector<double>& v) {
+  if (s.nrows != nr || s.ncols != nc)
+    return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": dimensions do not match the problem");
+  if (s.nnz < 0 || s.nnz > (int64_t)std::numeric_limits<int32_t>::max())
+    return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": nnz out of range");
+  if (nr > 0 && !s.rowptr) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": null rowptr");
+  if (s.nnz > 0 && (!s.colind || !s.values)) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": null arrays");
+  rp.resize(nr + 1);
+  ci.resize(s.nnz);
+  v.resize(s.nnz);
+  if (nr == 0) {
+    rp[0] = 0;
+    if (s.nnz != 0) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": nonzeros without rows");
+    return HPR_OK;
+  }
+  for (int64_t i = 0; i <= nr; ++i) rp[i] = s.rowptr[i] - base;
+  if (rp[0] != 0 || rp[nr] != s.nnz) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": rowptr does not span nnz");
+  for (int64_t i = 0; i < nr; ++i)
+    if (rp[i + 1] < rp[i]) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": rowptr decreases");
+  bool sorted = true;
+  for (int64_t i = 0; i < nr; ++i)
+    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+      int32_t j = s.colind[k] - base;
+      if (j < 0 || j >= nc) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": column index out of range");
+      double x = s.values[k];
+      if (!std::isfinite(x)) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": non-finite value");
+      ci[k] = j;
+      v[k] = x;
+      if (k > rp[i] && ci[k] < ci[k - 1]) sorted = false;
+    }
+  if (!sorted) {
+    // order each row by column, as Julia's SparseMatrixCSC always is
+    vector<std::pair<int32_t, double>> tmp;
+    for (int64_t i = 0; i < nr; ++i) {
+      tmp.clear();
+      for (int64_t k = rp[i]; k < rp[i + 1]; ++k) tmp.push_back({ci[k], v[k]});
+      std::stable_sort(tmp.begin(), tmp.end(),
+                       [](const std::pair<int32_t, double>& a, const std::pair<int32_t, double>& b) {
+                         return a.first < b.first;
+                       });
+      for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+        ci[k] = tmp[k - rp[i]].first;
+        v[k] = tmp[k - rp[i]].second;
+      }
+    }
+  }
+  return HPR_OK;
+}
+
+void transpose(int64_t nr, int64_t nc, const vector<int32_t>& rp, const vector<int32_t>& ci, const vector<double>& v,
+               vector<int32_t>& trp, vector<int32_t>& tci, vector<double>& tv) {
+  trp.assign(nc + 1, 0);
+  for (size_t k = 0; k < ci.size(); ++k) trp[ci[k] + 1]++;
+  for (int64_t j = 0; j < nc; ++j) trp[j + 1] += trp[j];
+  tci.resize(ci.size());
+  tv.resize(v.size());
+  vector<int32_t> pos(trp.begin(), trp.end() - 1);
+  for (int64_t i = 0; i < nr; ++i)
+    for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+      int32_t p = pos[ci[k]]++;
+      tci[p] = (int32_t)i;
+      tv[p] = v[k];
+    }
+}
+
+int put_csr(Ctx* c, DevCSR& M, int64_t nr, int64_t nc, const vector<int32_t>& rp, const vector<int32_t>& ci,
+            const vector<double>& v) {
+  M.nrows = nr;
+  M.ncols = nc;
+  M.nnz = (int64_t)ci.size();
+  HPR_TRY(dev_alloc_n(c, &M.rowptr, nr + 1));
+  HPR_TRY(dev_alloc_n(c, &M.col, M.nnz));
+  HPR_TRY(dev_alloc_n(c, &M.val, M.nnz));
+  HPR_CUDA(c, cudaMemcpy(M.rowptr, rp.data(), (nr + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (M.nnz) {
+    HPR_CUDA(c, cudaMemcpy(M.col, ci.data(), M.nnz * sizeof(int32_t), cudaMemcpyHostToDevice));
+    HPR_CUDA(c, cudaMemcpy(M.val, v.data(), M.nnz * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  return HPR_OK;
+}
+
+int put_vec(Ctx* c, double** d, const double* h, int64_t n) {
+  HPR_TRY(dev_alloc_n(c, d, n));
+  if (n > 0) {
+    if (h) HPR_CUDA(c, cudaMemcpy(*d, h, n * sizeof(double), cudaMemcpyHostToDevice));
+    else HPR_CUDA(c, cudaMemset(*d, 0, n * sizeof(double)));
+  }
+  return HPR_OK;
+}
+
+int zero_vec(Ctx* c, double** d, int64_t n) {
+  HPR_TRY(dev_alloc_n(c, d, n));
+  HPR_CUDA(c, cudaMemset(*d, 0, std::max<int64_t>(n, 1) * sizeof(double)));
+  return HPR_OK;
+}
+
+int cone_index(Ctx* c, const int64_t* idx, int64_t len, int base, int64_t first, int64_t last, const char* name,
+               vector<int64_t>& out) {
+  out.clear();
+  if (len <= 0 || !idx) {
+    out.push_back(last);
+    if (first != last) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": empty index but rows remain");
+    return HPR_OK;
+  }
+  for (int64_t k = 0; k < len; ++k) out.push_back(idx[k] - base);
+  if (out.front() != first) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": must start after the linear part");
+  if (out.back() != last) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": must end at the last row");
+  for (int64_t k = 0; k + 1 < (int64_t)out.size(); ++k)
+    if (out[k + 1] <= out[k]) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": cone sizes must be >= 1");
+  return HPR_OK;
+}
+
+const double kInf = std::numeric_limits<double>::infinity();
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host restatement of the solve loop (solve, algorithm.jl:2765-2905) with
+// check_restart (1016-1099), update_sigma! (729-990) and do_restart!
+// (1130-1166).  Vector work runs on the device; the host keeps the scalar
+// decisions, reading back a few reductions at each check.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct RestartInfo {
+  int flag = 0;
+  bool first = true;
+  double last_gap = kInf, current_gap = kInf, save_gap = kInf;
+  int64_t inner = 0;
+  int times = 0;
+  double weighted = kInf, best_gap = kInf, best_kkt = kInf, best_sigma = 1.0;
+  int64_t best_iter = 0;
+  bool corr_active = false;
+  int corr_dir = 0;
+};
+
+inline double jl_clamp(double x, double lo, double hi) { return x > hi ? hi : (x < lo ? lo : x); }
+
+double print_step(int64_t iter) {
+  double p = std::pow(10.0, std::floor(std::log10((double)iter))) / 10.0;
+  return std::max(p, 10.0);
+}
+
+bool is_print_iter(int64_t iter, const hpr_params* P) {
+  if (P->print_frequency == -1) return std::fmod((double)iter, print_step(iter)) == 0 || iter == P->max_iter;
+  return iter % P->print_frequency == 0 || iter == P->max_iter;
+}
+
+void check_restart(RestartInfo& R, int64_t iter, int64_t ci, double sigma, double kkt) {
+  R.flag = 0;
+  if (R.first) {
+    if (iter == ci) {
+      R.first = false;
+      R.flag = 1;
+      R.weighted = R.current_gap;
+      R.best_gap = R.current_gap;
+      R.best_kkt = kkt;
+      R.best_sigma = sigma;
+    }
+    return;
+  }
+  if (iter % ci != 0) return;
+  if (R.current_gap < 0) R.current_gap = 1e-6;
+  if (R.current_gap <= 0.36 * R.last_gap) R.flag = 1;
+  if (R.current_gap <= 0.8 * R.last_gap && R.current_gap > R.save_gap) R.flag = 2;
+  if ((R.inner >= std::max(500.0, 0.15 * (double)iter) || (R.inner >= 10000 && R.current_gap <= 0.75 * R.last_gap)) &&
+      R.current_gap > 0.9 * R.save_gap)
+    R.flag = 3;
+  // should_refresh_best_sigma (algorithm.jl:690-703)
+  bool improved = kkt < R.best_kkt;
+  bool compat = R.current_gap < R.best_gap && kkt <= 1.01 * R.best_kkt;
+  bool periodic = R.best_iter >= 10 && kkt <= 1.2 * R.best_kkt;
+  if (improved || compat || periodic) {
+    R.best_gap = R.current_gap;
+    R.best_kkt = kkt;
+    R.best_sigma = sigma;
+    R.best_iter = 0;
+  }
+  R.save_gap = R.current_gap;
+}
+
+// golden (kernels.jl:6268-6305): golden-section search of
+// a x + b/x + c x^2/(1 + d x) on [lo, hi].
+double golden_search(double ap, double bp, double cp, double dp, double lo, double hi, double tol) {
+  auto f = [&](double x) { return ap * x + bp / x + cp * (x * x) / (1 + dp * x); };
+  const double phi = (std::sqrt(5.0) - 1.0) / 2.0;
+  double a = lo, b = hi, c = b - phi * (b - a), d = a + phi * (b - a);
+  double fc = f(c), fd = f(d);
+  for (int i = 0; i < 200; ++i) {
+    if (fd < fc) {
+      a = c;
+      c = d;
+      fc = fd;
+      d = a + phi * (b - a);
+      fd = f(d);
+    } else {
+      b = d;
+      d = c;
+      fd = fc;
+      c = b - phi * (b - a);
+      fc = f(c);
+    }
+    if ((b - a) < tol) break;
+  }
+  return 0.5 * (a + b);
+}
+
+int update_sigma(Ctx* c, RestartInfo& R, const hpr_residuals& res) {
+  if (R.flag < 1) return HPR_OK;
+  const bool skipq = !c->has_q, has_m = c->m > 0;
+  const double s_old = c->sigma;
+  double a, b, cc, d;
+  HPR_TRY(launch_sigma_terms(c, &a, &b, &cc, &d));
+  a = std::max(a, 1e-16);
+  b = std::max(b, 1e-16);
+  double sm;
+  if (skipq || !has_m) sm = std::sqrt(b / a);
+  else if (c->Q_is_diag) HPR_TRY(launch_golden_diag(c, a, b, 1e-12, 1e12, 1e-13, &sm));
+  else sm = golden_search(a, b, cc, d, 1e-12, 1e12, 1e-13);
+  // historical stabilisation (algorithm.jl:873-885)
+  double ck = res.KKTx_and_gap_org_bar, cg = R.current_gap;
+  bool ref_ok = (ck <= 10.0 * R.best_kkt) && (cg <= 10.0 * R.best_gap);
+  double pr = jl_clamp(std::sqrt((ck / R.best_kkt) * (cg / R.best_gap)), 1.0, 10.0);
+  double base = sm;
+  if (ref_ok) {
+    double th = jl_clamp(std::exp(-0.3 * (pr - 1.0)), 0.0, 1.0);
+    base = jl_clamp(std::exp(th * std::log(sm) + (1.0 - th) * std::log(R.best_sigma)), 1e-12, 1e12);
+  }
+  // residual-imbalance correction (algorithm.jl:897-954)
+  const double THR = 1e-8;
+  double ep = std::max(res.err_Rp_org_bar, 1e-16), ed = std::max(res.err_Rd_org_bar, 1e-16);
+  double es = std::min(ep, ed), el = std::max(ep, ed), ir = el / es;
+  bool both = el <= THR;
+  bool one = es <= 0.5 * THR && el >= 2.0 * THR;
+  bool ext = ir >= 1e6;
+  bool trig = !both && (one || ext);
+  bool keep = !both && (es <= 0.8 * THR || ir >= 1e5);
+  if (!both && (trig || (R.corr_active && keep))) {
+    R.corr_active = true;
+    R.corr_dir = ed >= ep ? 1 : -1;
+  } else {
+    R.corr_active = false;
+    R.corr_dir = 0;
+  }
+  double beta = 0.0;
+  if (!both) {
+    if (one) beta = 0.5;
+    if (ext) beta = 1.0;
+    else if (R.corr_active) beta = 0.5;
+  }
+  double kappa = 1.0;
+  if (beta > 0.0) {
+    double rk = ed / ep;
+    if (R.corr_active) rk = R.corr_dir > 0 ? std::max(rk, 2.0) : std::min(rk, 0.5);
+    kappa = std::exp(beta * jl_clamp(std::log(rk), -std::log(100.0), std::log(100.0)));
+  }
+  double sn = base * kappa;
+  if (R.corr_active) sn = R.corr_dir > 0 ? std::max(sn, s_old * 1.5) : std::min(sn, s_old / 1.5);
+  sn = jl_clamp(sn, 1e-12, 1e12);
+  c->sigma = sn;
+  R.best_iter += 1;
+  if (c->Q_is_diag && !skipq && std::fabs(s_old - sn) > 1e-15) HPR_TRY(update_q_factors(c));
+  return push_state(c);
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Capture G partial iterations into a graph (launch-bound small problems).
+int capture_partial_graph(Ctx* c, int G) {
+  if (c->graph_partial) return HPR_OK;
+  cudaGraph_t g;
+  HPR_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = HPR_OK;
+  for (int i = 0; i < G && rc == HPR_OK; ++i) rc = launch_iteration(c, false);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (rc != HPR_OK) return rc;
+  if (e != cudaSuccess) return set_err(c, HPR_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&c->graph_partial, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return set_err(c, HPR_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  c->graph_iters = G;
+  return HPR_OK;
+}
+
+}  // namespace
+
+int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
+  if (P->sigma != -1 && !(P->sigma > 0)) return set_err(c, HPR_E_BAD_INPUT, "invalid sigma");
+  if (P->print_frequency != -1 && P->print_frequency <= 0) return set_err(c, HPR_E_BAD_INPUT, "invalid print_frequency");
+  if (P->check_iter <= 0) return set_err(c, HPR_E_BAD_INPUT, "invalid check_iter");
+  if (!c->scaled) HPR_TRY(run_scaling(c, P, nullptr));
+  // sigma (allocate_workspace, algorithm.jl:1531-1551)
+  double sigma = 1.0;
+  if (P->sigma == -1) {
+    if (c->norm_c > 1e-16 && c->norm_b > 1e-16 && c->norm_b < 1e16 && c->norm_c < 1e16) sigma = c->norm_b / c->norm_c;
+  } else {
+    sigma = P->sigma;
+  }
+  const double t0 = now_s();
+  double lamA = 0.0, lamQ = 0.0;
+  if (P->lambda_max_A > 0) lamA = P->lambda_max_A;
+  else if (c->m > 0) {
+    HPR_TRY(launch_power_A(c, 5000, 1e-4, &lamA));
+    lamA *= 1.05;
+  }
+  // compute_lambda_max_Q (unified_operations.jl:727-741)
+  if (P->lambda_max_Q > 0) lamQ = P->lambda_max_Q;
+  else if (c->has_q) {
+    if (c->q_kind == HPR_Q_DIAG_LOWRANK || !c->Q_is_diag) {
+      HPR_TRY(launch_power_Q(c, 5000, 1e-4, &lamQ));
+      lamQ *= 1.05;
+    } else {
+      vector<double> qv(c->Q.nnz);
+      HPR_CUDA(c, cudaMemcpy(qv.data(), c->Q.val, c->Q.nnz * sizeof(double), cudaMemcpyDeviceToHost));
+      lamQ = -kInf;
+      for (double v : qv) lamQ = std::max(lamQ, v);
+    }
+  }
+  const double power_time = now_s() - t0;
+  c->sigma = sigma;
+  c->lamA = lamA;
+  c->lamQ = lamQ;
+  c->inner = 0;
+  HPR_TRY(push_state(c));
+  HPR_TRY(update_q_factors(c));
+  if (P->initial_x || P->initial_y) HPR_TRY(launch_initial_points(c, P->initial_x, P->initial_y));
+  // small problems are launch-bound: replay captured partial iterations
+  if (c->A.nnz + c->n + c->m < (int64_t)4000000) HPR_TRY(capture_partial_graph(c, 8));
+
+  RestartInfo R;
+  R.best_sigma = c->sigma;
+  hpr_residuals rs;
+  std::memset(&rs, 0, sizeof(rs));
+  int64_t iter_4 = 0, iter_6 = 0;
+  double time_4 = 0, time_6 = 0;
+  const int64_t ci = P->check_iter;
+  int status = -1;
+  int64_t iter = 0;
+  if (P->verbose) std::printf(" iter     errRp     errRd         p_obj           d_obj          gap        sigma       time\n");
+  while (true) {
+    // ---- the event iteration `iter` (residual check or print)
+    double el = now_s() - t0;
+    bool print_yes = is_print_iter(iter, P) || el > P->time_limit;
+    if (iter % ci == 0 || print_yes) HPR_TRY(launch_residuals(c, iter == 0, &rs));
+    if (rs.KKTx_and_gap_org_bar != rs.KKTx_and_gap_org_bar)
+      return set_err(c, HPR_E_NUMERIC, "NaN in the KKT residuals at iteration " + std::to_string(iter));
+    if (rs.KKTx_and_gap_org_bar < P->stoptol) status = HPR_STATUS_OPTIMAL;
+    else if (iter == P->max_iter) status = HPR_STATUS_MAX_ITER;
+    else if (now_s() - t0 > P->time_limit) status = HPR_STATUS_TIME_LIMIT;
+    check_restart(R, iter, ci, c->sigma, rs.KKTx_and_gap_org_bar);
+    HPR_TRY(update_sigma(c, R, rs));
+    if (R.flag > 0) {
+      HPR_TRY(launch_restart(c));
+      R.last_gap = R.current_gap;
+      R.save_gap = kInf;
+      R.times++;
+      R.inner = 0;
+    }
+    if (P->verbose && (print_yes || status >= 0))
+      std::printf("%5lld    %3.2e    %3.2e    %+7.6e    %+7.6e    %3.2e    %3.2e    %6.2f\n", (long long)iter,
+                  rs.err_Rp_org_bar, rs.err_Rd_org_bar, rs.primal_obj_bar, rs.dual_obj_bar, rs.rel_gap_bar, c->sigma,
+                  now_s() - t0);
+    if (rs.KKTx_and_gap_org_bar < 1e-4 && iter_4 == 0 && time_4 == 0) {
+      time_4 = now_s() - t0;
+      iter_4 = iter;
+      if (iter == 0) time_4 = 1e-300;
+    }
+    if (rs.KKTx_and_gap_org_bar < 1e-6 && iter_6 == 0 && time_6 == 0) {
+      time_6 = now_s() - t0;
+      iter_6 = iter;
+      if (iter == 0) time_6 = 1e-300;
+    }
+    if (status >= 0) break;
+    // ---- steps up to the next event (perform_iteration_step!, algorithm.jl:2722-2744)
+    int64_t next = iter + 1;
+    while (!(next % ci == 0 || is_print_iter(next, P))) ++next;
+    if (R.flag > 0) {
+      // the restart iteration's own step is full and needs the M-norm
+      HPR_TRY(run_iterations(c, 1, true));
+      double mn;
+      HPR_TRY(launch_mnorm(c, &mn));
+      R.last_gap = std::min(mn, R.last_gap);
+      if ((iter + 1) % ci == 0) R.current_gap = mn;
+      R.inner += 1;
+      iter += 1;
+      if (iter < next) {
+        HPR_TRY(run_iterations(c, next - iter, true));
+        R.inner += next - iter;
+        if (next % ci == 0) HPR_TRY(launch_mnorm(c, &R.current_gap));
+      }
+    } else {
+      HPR_TRY(run_iterations(c, next - iter, true));
+      R.inner += next - iter;
+      if (next % ci == 0) HPR_TRY(launch_mnorm(c, &R.current_gap));
+    }
+    iter = next;
+  }
+  const double tt = now_s() - t0;
+  if (out) {
+    out->iter = iter;
+    out->time = tt;
+    out->power_time = power_time;
+    out->residuals = rs.KKTx_and_gap_org_bar;
+    out->primal_obj = rs.primal_obj_bar;
+    out->gap = rs.rel_gap_bar;
+    out->status = status;
+    out->restarts = R.times;
+    out->time_4 = time_4 == 0.0 ? tt : (time_4 < 1e-200 ? 0.0 : time_4);
+    out->iter_4 = (iter_4 == 0 && time_4 == 0.0) ? iter : iter_4;
+    out->time_6 = time_6 == 0.0 ? tt : (time_6 < 1e-200 ? 0.0 : time_6);
+    out->iter_6 = (iter_6 == 0 && time_6 == 0.0) ? iter : iter_6;
+    out->sigma_final = c->sigma;
+    out->lambda_max_A = lamA;
+    out->lambda_max_Q = lamQ;
+    out->last = rs;
+    HPR_TRY(launch_unscale(c, out->x, out->y, out->z, out->w));
+  }
+  return HPR_OK;
+}
+
+}  // namespace hpr
+
+using namespace hpr;
+
+namespace {
+Ctx* C(hpr_ctx* h) { return &h->c; }
+int need_upload(Ctx* c) { return c->uploaded ? HPR_OK : set_err(c, HPR_E_STATE, "no problem uploaded"); }
+
+int vec_ptr(Ctx* c, int which, double** p, int64_t* len) {
+  const int64_t n = c->n, m = c->m;
+  switch (which) {
+    case HPR_VEC_X: *p = c->x; *len = n; break;
+    case HPR_VEC_X_BAR: *p = c->x_bar; *len = n; break;
+    case HPR_VEC_X_HAT: *p = c->x_hat; *len = n; break;
+    case HPR_VEC_LAST_X: *p = c->last_x; *len = n; break;
+    case HPR_VEC_Z_BAR: *p = c->z_bar; *len = n; break;
+    case HPR_VEC_Y: *p = c->y; *len = m; break;
+    case HPR_VEC_Y_BAR: *p = c->y_bar; *len = m; break;
+    case HPR_VEC_LAST_Y: *p = c->last_y; *len = m; break;
+    case HPR_VEC_S: *p = c->s; *len = m; break;
+    case HPR_VEC_W: *p = c->w; *len = n; break;
+    case HPR_VEC_W_BAR: *p = c->w_bar; *len = n; break;
+    case HPR_VEC_LAST_W: *p = c->last_w; *len = n; break;
+    case HPR_VEC_ATY: *p = c->ATy; *len = n; break;
+    case HPR_VEC_LAST_ATY: *p = c->last_ATy; *len = n; break;
+    case HPR_VEC_DX: *p = c->dx; *len = n; break;
+    case HPR_VEC_DY: *p = c->dy; *len = m; break;
+    case HPR_VEC_ROW_NORM: *p = c->row_norm; *len = m; break;
+    case HPR_VEC_COL_NORM: *p = c->col_norm; *len = n; break;
+    case HPR_VEC_C: *p = c->c; *len = n; break;
+    case HPR_VEC_AL: *p = c->AL; *len = m; break;
+    case HPR_VEC_AU: *p = c->AU; *len = m; break;
+    case HPR_VEC_L: *p = c->l; *len = n; break;
+    case HPR_VEC_U: *p = c->u; *len = n; break;
+    case HPR_VEC_SOC_RHS: *p = c->soc_rhs; *len = m - c->m_lin; break;
+    case HPR_VEC_A_VALUES: *p = c->A.val; *len = c->A.nnz; break;
+    case HPR_VEC_AT_VALUES: *p = c->AT.val; *len = c->AT.nnz; break;
+    case HPR_VEC_DW: *p = c->dw; *len = n; break;
+    default: return set_err(c, HPR_E_BAD_INPUT, "unknown vector id");
+  }
+  return HPR_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int hpr_version(void) { return 10000; }
+
+const char* hpr_status_string(int code) {
+  switch (code) {
+    case HPR_OK: return "ok";
+    case HPR_E_CUDA: return "CUDA error or no usable device";
+    case HPR_E_BUDGET: return "HBM budget exceeded";
+    case HPR_E_BAD_INPUT: return "bad input";
+    case HPR_E_NUMERIC: return "numerical failure (NaN/Inf)";
+    case HPR_E_TIMEOUT: return "device wait timed out";
+    case HPR_E_STATE: return "invalid call order";
+    case HPR_E_UNSUPPORTED: return "unsupported";
+  }
+  return "unknown status";
+}
+
+void hpr_default_params(hpr_params* p) {
+  // HPRSOCP_parameters() (src/structs.jl:277)
+  std::memset(p, 0, sizeof(*p));
+  p->stoptol = 1e-6;
+  p->sigma = -1;
+  p->max_iter = 2147483647;
+  p->time_limit = 3600.0;
+  p->check_iter = 150;
+  p->print_frequency = -1;
+  p->use_Ruiz_scaling = 1;
+  p->ruiz_iterations = 10;
+  p->use_bc_scaling = 1;
+  p->bc_scaling_norm_type = HPR_BC_NORM_L2;
+  p->use_Pock_Chambolle_scaling = 1;
+  p->soc_block_scaling_strategy = HPR_SOC_SCALE_PHASE_TAPER;
+  p->verbose = 0;
+  p->lambda_max_A = -1;
+  p->lambda_max_Q = -1;
+  p->precision = HPR_PREC_FP64;
+  p->refine = 0;
+}
+
+int hpr_create(int device, size_t budget, hpr_ctx** out) {
+  if (!out) return HPR_E_BAD_INPUT;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return HPR_E_CUDA;
+  if (device < 0 || device >= ndev) return HPR_E_BAD_INPUT;
+  if (cudaSetDevice(device) != cudaSuccess) return HPR_E_CUDA;
+  hpr_ctx* h = new hpr_ctx();
+  Ctx* c = &h->c;
+  c->device = device;
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    delete h;
+    return HPR_E_CUDA;
+  }
+  c->budget = budget ? budget : (size_t)(0.9 * (double)fr);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaMallocHost(&c->h_red_out, 64 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&c->h_state, sizeof(DevState)) != cudaSuccess) {
+    delete h;
+    return HPR_E_CUDA;
+  }
+  *out = h;
+  return HPR_OK;
+}
+
+int hpr_destroy(hpr_ctx* h) {
+  if (!h) return HPR_OK;
+  Ctx* c = C(h);
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_all(c);
+  if (c->h_red_out) cudaFreeHost(c->h_red_out);
+  if (c->h_state) cudaFreeHost(c->h_state);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete h;
+  return HPR_OK;
+}
+
+const char* hpr_last_error(const hpr_ctx* h) { return h ? h->c.err.c_str() : "null context"; }
+
+int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
+  if (!h || !p) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  cudaSetDevice(c->device);
+  free_all(c);
+  const int base = p->index_base;
+  if (base != 0 && base != 1) return set_err(c, HPR_E_BAD_INPUT, "index_base must be 0 or 1");
+  const int64_t m = p->m, n = p->n;
+  if (m < 0 || n < 0 || p->m_lin < 0 || p->m_lin > m || p->n_box < 0 || p->n_box > n)
+    return set_err(c, HPR_E_BAD_INPUT, "invalid dimensions");
+  if (m > (int64_t)std::numeric_limits<int32_t>::max() - 1 || n > (int64_t)std::numeric_limits<int32_t>::max() - 1)
+    return set_err(c, HPR_E_BAD_INPUT, "dimensions exceed the int32 index range");
+  if ((n > 0 && (!p->c || !p->l || !p->u)) || (m > 0 && (!p->AL || !p->AU)))
+    return set_err(c, HPR_E_BAD_INPUT, "null problem vector");
+  c->m = m;
+  c->n = n;
+  c->m_lin = p->m_lin;
+  c->n_box = p->n_box;
+  c->obj_constant = p->obj_constant;
+  if (!std::isfinite(p->obj_constant)) return set_err(c, HPR_E_BAD_INPUT, "non-finite objective constant");
+  if (!finite_all(p->c, n)) return set_err(c, HPR_E_BAD_INPUT, "c has non-finite entries");
+  if (!nonan_all(p->l, n) || !nonan_all(p->u, n) || !nonan_all(p->AL, m) || !nonan_all(p->AU, m))
+    return set_err(c, HPR_E_BAD_INPUT, "NaN in bounds");
+  if (m - p->m_lin > 0 && p->soc_rhs && !finite_all(p->soc_rhs, m - p->m_lin))
+    return set_err(c, HPR_E_BAD_INPUT, "soc_rhs has non-finite entries");
+  HPR_TRY(cone_index(c, p->soc_con_idx, p->n_soc_con_idx, base, p->m_lin, m, "soc_con_idx", c->h_con_idx));
+  int64_t nbox = p->n_box;
+  if (p->n_soc_var_idx > 1) {
+    HPR_TRY(cone_index(c, p->soc_var_idx, p->n_soc_var_idx, base, nbox, n, "soc_var_idx", c->h_var_idx));
+  } else {
+    c->h_var_idx.assign(1, n);
+  }
+  // A and A'
+  vector<int32_t> rp, ci, trp, tci;
+  vector<double> v, tv;
+  HPR_TRY(load_csr(c, p->A, base, m, n, "A", rp, ci, v));
+  if (p->AT.rowptr) HPR_TRY(load_csr(c, p->AT, base, n, m, "AT", trp, tci, tv));
+  else transpose(m, n, rp, ci, v, trp, tci, tv);
+  if ((int64_t)tci.size() != (int64_t)ci.size()) return set_err(c, HPR_E_BAD_INPUT, "AT nnz differs from A");
+  HPR_TRY(put_csr(c, c->A, m, n, rp, ci, v));
+  HPR_TRY(put_csr(c, c->AT, n, m, trp, tci, tv));
+  c->h_A_rowptr = rp;
+  c->h_AT_rowptr = trp;
+  // Q
+  c->q_kind = p->q_kind;
+  c->has_q = false;
+  vector<int32_t> qrp, qci;
+  vector<double> qv;
+  if (p->q_kind == HPR_Q_CSR) {
+    HPR_TRY(load_csr(c, p->Q, base, n, n, "Q", qrp, qci, qv));
+    if (qci.empty()) {
+      c->q_kind = HPR_Q_NONE;
+    } else {
+      c->has_q = true;
+      HPR_TRY(put_csr(c, c->Q, n, n, qrp, qci, qv));
+    }
+  } else if (p->q_kind == HPR_Q_DIAG_LOWRANK) {
+    if (!p->q_diag) return set_err(c, HPR_E_BAD_INPUT, "q_diag is null");
+    if (!finite_all(p->q_diag, n)) return set_err(c, HPR_E_BAD_INPUT, "q_diag has non-finite entries");
+    int64_t k = p->F.nrows;
+    vector<int32_t> frp, fci, ftrp, ftci;
+    vector<double> fv, ftv;
+    HPR_TRY(load_csr(c, p->F, base, k, n, "F", frp, fci, fv));
+    transpose(k, n, frp, fci, fv, ftrp, ftci, ftv);
+    HPR_TRY(put_csr(c, c->F, k, n, frp, fci, fv));
+    HPR_TRY(put_csr(c, c->FT, n, k, ftrp, ftci, ftv));
+    HPR_TRY(put_vec(c, &c->qdiag, p->q_diag, n));
+    c->has_q = true;
+    qrp = ftrp;
+    build_plan(frp, k, {}, c->planF);
+    HPR_TRY(upload_plan(c, c->planF));
+  } else if (p->q_kind != HPR_Q_NONE) {
+    return set_err(c, HPR_E_BAD_INPUT, "unknown q_kind");
+  }
+  // cone index copies (int32)
+  {
+    vector<int32_t> cs(c->h_con_idx.begin(), c->h_con_idx.end()), vs(c->h_var_idx.begin(), c->h_var_idx.end());
+    HPR_TRY(dev_alloc_n(c, &c->d_con_start, (int64_t)cs.size()));
+    HPR_TRY(dev_alloc_n(c, &c->d_var_start, (int64_t)vs.size()));
+    HPR_CUDA(c, cudaMemcpy(c->d_con_start, cs.data(), cs.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    HPR_CUDA(c, cudaMemcpy(c->d_var_start, vs.data(), vs.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  // plans
+  vector<int64_t> vcones = c->h_var_idx.size() > 1 ? c->h_var_idx : vector<int64_t>();
+  vector<int64_t> ccones = c->h_con_idx.size() > 1 ? c->h_con_idx : vector<int64_t>();
+  build_plan(trp, n, vcones, c->planX);
+  build_plan(rp, m, ccones, c->planY);
+  HPR_TRY(upload_plan(c, c->planX));
+  HPR_TRY(upload_plan(c, c->planY));
+  if (c->has_q) {
+    build_plan(qrp, n, vcones, c->planQ);
+    HPR_TRY(upload_plan(c, c->planQ));
+  }
+  // problem vectors
+  HPR_TRY(put_vec(c, &c->c, p->c, n));
+  HPR_TRY(put_vec(c, &c->l, p->l, n));
+  HPR_TRY(put_vec(c, &c->u, p->u, n));
+  HPR_TRY(put_vec(c, &c->AL, p->AL, m));
+  HPR_TRY(put_vec(c, &c->AU, p->AU, m));
+  HPR_TRY(put_vec(c, &c->soc_rhs, p->soc_rhs, m - p->m_lin));
+  {
+    vector<double> full(m, 0.0);
+    if (p->soc_rhs)
+      for (int64_t i = p->m_lin; i < m; ++i) full[i] = p->soc_rhs[i - p->m_lin];
+    HPR_TRY(put_vec(c, &c->soc_rhs_full, full.data(), m));
+  }
+  // workspace (allocate_workspace, algorithm.jl:1443-1588)
+  double** nvecs[] = {&c->row_norm, &c->col_norm, &c->diag_Q, &c->fact1, &c->fact2, &c->fact,  &c->fact_M,
+                      &c->x,        &c->x_hat,    &c->x_bar,  &c->last_x, &c->z_bar, &c->dx,   &c->w,
+                      &c->w_bar,    &c->last_w,   &c->dw,     &c->Qw,     &c->dQw,   &c->Qx,   &c->tempv,
+                      &c->ATy,      &c->ATy_bar,  &c->last_ATy, &c->ATdy, &c->QATdy, &c->Rd,   &c->vtmp_n,
+                      &c->ptq};
+  for (double** v2 : nvecs) HPR_TRY(zero_vec(c, v2, n));
+  double** mvecs[] = {&c->y, &c->y_bar, &c->last_y, &c->s, &c->dy, &c->Rp, &c->Ax, &c->vtmp_m};
+  for (double** v2 : mvecs) HPR_TRY(zero_vec(c, v2, m));
+  HPR_TRY(zero_vec(c, &c->pz, std::max(m, n)));
+  HPR_TRY(zero_vec(c, &c->pq, std::max(m, n)));
+  int64_t kF = c->F.nrows;
+  HPR_TRY(zero_vec(c, &c->ftmp, kF));
+  HPR_TRY(zero_vec(c, &c->ftmp2, kF));
+  HPR_TRY(dev_alloc_n(c, &c->g32_n, n));
+  HPR_TRY(dev_alloc_n(c, &c->g32_m, m));
+  HPR_TRY(zero_vec(c, &c->d_red_out, 64));
+  int64_t need = (int64_t)kRedGrid * kMaxRed;
+  if (need > c->red_slots) {
+    if (c->d_red) cudaFree(c->d_red);
+    HPR_TRY(dev_alloc_n(c, &c->d_red, need));
+    c->red_slots = need;
+  }
+  {
+    double *rn = c->row_norm, *cn = c->col_norm;
+    HPR_TRY(vec_map(c, m, [=] __device__(int64_t i) { rn[i] = 1.0; }));
+    HPR_TRY(vec_map(c, n, [=] __device__(int64_t i) { cn[i] = 1.0; }));
+  }
+  HPR_TRY(dev_alloc_n(c, &c->d_state, 1));
+  c->sigma = 1.0;
+  c->lamA = c->lamQ = 0.0;
+  c->inner = 0;
+  c->b_scale = c->c_scale = 1.0;
+  c->precision = HPR_PREC_FP64;
+  HPR_TRY(push_state(c));
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->uploaded = true;
+  c->scaled = false;
+  return HPR_OK;
+}
+
+int hpr_scale(hpr_ctx* h, const hpr_params* opts, hpr_scale_info* out) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  if (c->scaled) return set_err(c, HPR_E_STATE, "problem already scaled");
+  hpr_params d;
+  if (!opts) {
+    hpr_default_params(&d);
+    opts = &d;
+  }
+  cudaSetDevice(c->device);
+  return run_scaling(c, opts, out);
+}
+
+int hpr_power_A(hpr_ctx* h, int maxit, double tol, double* lam) {
+  if (!h || !lam) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  return launch_power_A(c, maxit, tol, lam);
+}
+
+int hpr_power_Q(hpr_ctx* h, int maxit, double tol, double* lam) {
+  if (!h || !lam) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  return launch_power_Q(c, maxit, tol, lam);
+}
+
+int hpr_set_sigma_lambda(hpr_ctx* h, double sigma, double lamA, double lamQ) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  if (!(sigma > 0) || !std::isfinite(sigma)) return set_err(c, HPR_E_BAD_INPUT, "sigma must be positive");
+  c->sigma = sigma;
+  c->lamA = lamA;
+  c->lamQ = lamQ;
+  HPR_TRY(push_state(c));
+  HPR_TRY(update_q_factors(c));
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  return HPR_OK;
+}
+
+int hpr_set_inner(hpr_ctx* h, int64_t inner) {
+  if (!h || inner < 0) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  c->inner = inner;
+  return push_state(c);
+}
+
+int hpr_get_scalars(hpr_ctx* h, double* sigma, double* lamA, double* lamQ, int64_t* inner) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  if (sigma) *sigma = c->sigma;
+  if (lamA) *lamA = c->lamA;
+  if (lamQ) *lamQ = c->lamQ;
+  if (inner) *inner = c->inner;
+  return HPR_OK;
+}
+
+int hpr_iterate(hpr_ctx* h, int64_t k, int full_last) {
+  if (!h || k < 0) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  if (c->m > 0 && !(c->lamA > 0)) return set_err(c, HPR_E_STATE, "lambda_A must be set before iterating");
+  HPR_TRY(run_iterations(c, k, full_last != 0));
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  float ms = 0;
+  if (k > 0) cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  c->last_ms = ms;
+  return HPR_OK;
+}
+
+int hpr_compute_residuals(hpr_ctx* h, int include_bounds, hpr_residuals* out) {
+  if (!h || !out) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  return launch_residuals(c, include_bounds != 0, out);
+}
+
+int hpr_mnorm(hpr_ctx* h, double* out) {
+  if (!h || !out) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  return launch_mnorm(c, out);
+}
+
+int hpr_sigma_terms(hpr_ctx* h, double* a, double* b, double* cc, double* d) {
+  if (!h || !a || !b || !cc || !d) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  return launch_sigma_terms(c, a, b, cc, d);
+}
+
+int hpr_sigma_golden_diag(hpr_ctx* h, double a, double b, double lo, double hi, double tol, double* out) {
+  if (!h || !out) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  if (!c->Q_is_diag || !c->has_q) return set_err(c, HPR_E_STATE, "golden search over diag(Q) needs a diagonal Q");
+  return launch_golden_diag(c, a, b, lo, hi, tol, out);
+}
+
+int hpr_restart(hpr_ctx* h) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  HPR_TRY(launch_restart(c));
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  return HPR_OK;
+}
+
+int hpr_get_vector(hpr_ctx* h, int which, double* host, size_t len) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  double* p = nullptr;
+  int64_t L = 0;
+  HPR_TRY(vec_ptr(c, which, &p, &L));
+  if ((int64_t)len != L) return set_err(c, HPR_E_BAD_INPUT, "vector length mismatch");
+  if (L > 0) {
+    if (!host) return HPR_E_BAD_INPUT;
+    HPR_CUDA(c, cudaMemcpyAsync(host, p, L * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  return HPR_OK;
+}
+
+int hpr_set_vector(hpr_ctx* h, int which, const double* host, size_t len) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  double* p = nullptr;
+  int64_t L = 0;
+  HPR_TRY(vec_ptr(c, which, &p, &L));
+  if ((int64_t)len != L) return set_err(c, HPR_E_BAD_INPUT, "vector length mismatch");
+  if (which == HPR_VEC_A_VALUES || which == HPR_VEC_AT_VALUES)
+    if (!finite_all(host, L)) return set_err(c, HPR_E_BAD_INPUT, "non-finite matrix value");
+  if (L > 0) {
+    if (!host) return HPR_E_BAD_INPUT;
+    HPR_CUDA(c, cudaMemcpyAsync(p, host, L * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  if (c->precision != HPR_PREC_FP64 && (which == HPR_VEC_Y || which == HPR_VEC_A_VALUES || which == HPR_VEC_AT_VALUES))
+    HPR_TRY(repack_values(c));
+  return HPR_OK;
+}
+
+int hpr_get_solution(hpr_ctx* h, double* x, double* y, double* z, double* w) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  return launch_unscale(c, x, y, z, w);
+}
+
+int hpr_set_precision(hpr_ctx* h, int mode) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  if (mode != HPR_PREC_FP64 && mode != HPR_PREC_FP32 && mode != HPR_PREC_BF16)
+    return set_err(c, HPR_E_BAD_INPUT, "unknown precision mode");
+  c->precision = mode;
+  if (c->graph_partial) {
+    cudaGraphExecDestroy(c->graph_partial);
+    c->graph_partial = nullptr;
+    c->graph_iters = 0;
+  }
+  if (mode != HPR_PREC_FP64) HPR_TRY(repack_values(c));
+  return HPR_OK;
+}
+
+int hpr_solve(hpr_ctx* h, const hpr_params* params, hpr_results* res) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  hpr_params d;
+  if (!params) {
+    hpr_default_params(&d);
+    params = &d;
+  }
+  cudaSetDevice(c->device);
+  return solve_loop(c, params, res);
+}
+
+int hpr_optimize(const hpr_problem* prob, const hpr_params* params, hpr_results* res) {
+  hpr_params d;
+  if (!params) {
+    hpr_default_params(&d);
+    params = &d;
+  }
+  hpr_ctx* h = nullptr;
+  int rc = hpr_create(params->device_number, 0, &h);
+  if (rc != HPR_OK) return rc;
+  rc = hpr_upload(h, prob);
+  if (rc == HPR_OK) rc = hpr_solve(h, params, res);
+  if (rc != HPR_OK && params->verbose) std::fprintf(stderr, "hpr_optimize: %s\n", hpr_last_error(h));
+  hpr_destroy(h);
+  return rc;
+}
+
+int hpr_last_iterate_ms(hpr_ctx* h, double* ms, int64_t* launches) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  if (ms) *ms = c->last_ms;
+  if (launches) *launches = c->last_launches;
+  return HPR_OK;
+}
+
+int hpr_iteration_bytes(hpr_ctx* h, double* bytes) {
+  if (!h || !bytes) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  *bytes = iteration_bytes(c);
+  return HPR_OK;
+}
+
+}  // extern "C"

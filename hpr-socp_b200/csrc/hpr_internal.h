@@ -1,0 +1,230 @@
+// hpr_internal.h — internal types of the B200 HPR-SOCP library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/hprsocp_b200.h"
+
+namespace hpr {
+
+// ---------------------------------------------------------------------------
+// Tiling of the fused SpMV + epilogue engine.
+//   A CTA of kThreads threads processes one Task.  kNnzTile products are
+//   staged in shared memory and each row is summed in column order, so the
+//   result of a row whose nonzeros fit one tile is bit-identical to the
+//   reference's sequential CSC/CSR accumulation.
+// ---------------------------------------------------------------------------
+constexpr int kThreads = 256;
+constexpr int kNnzTile = 2048;
+constexpr int kRowCap = 1024;
+constexpr int kSerialMax = 64;      // rows longer than this use a warp reduction
+constexpr int kSmallConeMax = 128;  // larger cones take the multi-CTA path
+constexpr int kMaxRed = 8;          // reduction lanes per engine launch
+
+enum TaskKind : int16_t {
+  TASK_ROWS = 0,       // complete rows [rb,re); whole cones when cone >= 0
+  TASK_CONE_PART = 1,  // complete rows inside one big cone
+  TASK_LONG_PART = 2,  // a nonzero sub-range of one long row
+};
+
+struct Task {
+  int32_t rb, re;    // rows
+  int32_t nzb, nze;  // nonzero range
+  int16_t kind;
+  int16_t ncones;    // TASK_ROWS: number of whole cones in the task
+  int32_t cone;      // first cone (TASK_ROWS), the cone (CONE_PART), or -1
+  int32_t group;     // big-cone slot (CONE_PART) / long-row slot (LONG_PART)
+  int32_t part;      // part index within the long row (LONG_PART)
+};
+static_assert(sizeof(Task) == 32, "Task layout");
+
+struct BigCone {
+  int32_t cone, rb, re, nparts;
+};
+struct LongRow {
+  int32_t row, nparts, partial_base, bigcone;  // bigcone slot or -1
+};
+
+struct Plan {
+  int64_t nrows = 0;
+  std::vector<Task> tasks;
+  std::vector<BigCone> big;
+  std::vector<LongRow> lng;
+  int32_t npartials = 0;  // long-row partial sums
+  // device copies
+  Task* d_tasks = nullptr;
+  BigCone* d_big = nullptr;
+  LongRow* d_lng = nullptr;
+  int32_t* d_big_cnt = nullptr;
+  int32_t* d_lng_cnt = nullptr;
+  double* d_partials = nullptr;  // long-row partial sums
+  double* d_raw = nullptr;       // big-cone raw values (nrows)
+  int32_t nslots() const {
+    return (int32_t)tasks.size() + (int32_t)big.size() + (int32_t)lng.size();
+  }
+};
+
+// Build the task list of one matrix side.  `cone_starts` holds the first row
+// of every cone plus an end sentinel (empty when the side has no cones);
+// rows before cone_starts[0] are linear rows.
+void build_plan(const std::vector<int32_t>& rowptr, int64_t nrows,
+                const std::vector<int64_t>& cone_starts, Plan& plan);
+
+struct DevCSR {
+  int64_t nrows = 0, ncols = 0, nnz = 0;
+  int32_t* rowptr = nullptr;
+  int32_t* col = nullptr;
+  double* val = nullptr;
+  float* val32 = nullptr;
+  __nv_bfloat16* val16 = nullptr;
+};
+
+// Scalars read by the kernels; lives in device memory so captured graphs stay
+// valid across sigma updates and restarts.
+struct DevState {
+  double sigma;
+  double lamA;
+  double lamQ;
+  double pad0;
+  long long inner;
+  int32_t ticket;
+  int32_t error;
+};
+
+// Views of a matrix plan for a kernel launch.
+struct PlanView {
+  const Task* tasks;
+  const BigCone* big;
+  const LongRow* lng;
+  int32_t* big_cnt;
+  int32_t* lng_cnt;
+  double* partials;
+  double* raw;
+  const int32_t* cone_start;  // cone start rows (+ sentinel), this side
+  int32_t ntasks, nbig, nlng;
+};
+
+struct Ctx {
+  std::string err;
+  int device = 0;
+  size_t budget = 0, used = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool uploaded = false, scaled = false;
+  // problem
+  int64_t m = 0, n = 0, m_lin = 0, n_box = 0;
+  int q_kind = HPR_Q_NONE;
+  bool has_q = false, Q_is_diag = false;
+  DevCSR A, AT, Q, F, FT;
+  std::vector<int32_t> h_A_rowptr, h_AT_rowptr;
+  std::vector<int64_t> h_con_idx, h_var_idx;  // 0-based starts + sentinel
+  int32_t* d_con_start = nullptr;  // int32 copies (+ sentinel)
+  int32_t* d_var_start = nullptr;
+  double obj_constant = 0.0;
+  Plan planX, planY, planQ, planF;
+  // problem vectors (scaled in place by hpr_scale)
+  double *c = nullptr, *l = nullptr, *u = nullptr, *AL = nullptr,
+         *AU = nullptr, *soc_rhs = nullptr, *soc_rhs_full = nullptr,
+         *qdiag = nullptr;
+  // scaling
+  double *row_norm = nullptr, *col_norm = nullptr;
+  double b_scale = 1, c_scale = 1, norm_b = 0, norm_c = 0, norm_b_org = 0,
+         norm_c_org = 0;
+  double* diag_Q = nullptr;
+  double *fact1 = nullptr, *fact2 = nullptr, *fact = nullptr,
+         *fact_M = nullptr;
+  // workspace
+  double *x = nullptr, *x_hat = nullptr, *x_bar = nullptr, *last_x = nullptr,
+         *z_bar = nullptr, *dx = nullptr;
+  double *y = nullptr, *y_bar = nullptr, *last_y = nullptr, *s = nullptr,
+         *dy = nullptr;
+  double *w = nullptr, *w_bar = nullptr, *last_w = nullptr, *dw = nullptr,
+         *Qw = nullptr, *dQw = nullptr, *Qx = nullptr, *tempv = nullptr;
+  double *ATy = nullptr, *ATy_bar = nullptr, *last_ATy = nullptr,
+         *ATdy = nullptr, *QATdy = nullptr;
+  double *Rp = nullptr, *Rd = nullptr, *Ax = nullptr;
+  double* ftmp = nullptr;   // F v (k)
+  double* ftmp2 = nullptr;  // F w_bar (k)
+  double* vtmp_n = nullptr;
+  double* vtmp_m = nullptr;
+  float* g32_n = nullptr;  // FP32 copies of gathered vectors (x_hat/tempv, y)
+  float* g32_m = nullptr;
+  double *pz = nullptr, *pq = nullptr, *ptq = nullptr;  // power iteration
+  // reductions
+  double* d_red = nullptr;      // partial slots
+  int64_t red_slots = 0;
+  double* d_red_out = nullptr;  // final results (kMaxRed * 2)
+  double* h_red_out = nullptr;  // pinned
+  DevState* d_state = nullptr;
+  DevState* h_state = nullptr;  // pinned staging
+  // host mirrors
+  double sigma = 1, lamA = 0, lamQ = 0;
+  int64_t inner = 0;
+  int precision = HPR_PREC_FP64;
+  // graphs
+  cudaGraphExec_t graph_partial = nullptr;
+  int graph_iters = 0;
+  // timing
+  double last_ms = 0;
+  int64_t last_launches = 0;
+  int64_t launches = 0;
+};
+
+// error helpers
+int set_err(Ctx* c, int code, const std::string& msg);
+#define HPR_CUDA(ctx, call)                                                 \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess)                                                  \
+      return ::hpr::set_err((ctx), HPR_E_CUDA,                              \
+                            std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+#define HPR_TRY(...)                 \
+  do {                               \
+    int rc_ = (__VA_ARGS__);         \
+    if (rc_ != HPR_OK) return rc_;   \
+  } while (0)
+
+int dev_alloc(Ctx* c, void** p, size_t bytes);
+template <class T>
+int dev_alloc_n(Ctx* c, T** p, int64_t n) {
+  return dev_alloc(c, (void**)p, (size_t)(n > 0 ? n : 1) * sizeof(T));
+}
+
+// kernel launchers (hpr_kernels.cu)
+int upload_plan(Ctx* c, Plan& p);
+PlanView view_of(const Plan& p, const int32_t* cone_start);
+int launch_iteration(Ctx* c, bool full);
+int run_iterations(Ctx* c, int64_t k, bool full_last);
+int launch_residuals(Ctx* c, bool include_bounds, hpr_residuals* out);
+int launch_mnorm(Ctx* c, double* out);
+int launch_sigma_terms(Ctx* c, double* a, double* b, double* cc, double* d);
+int launch_golden_diag(Ctx* c, double a, double b, double lo, double hi,
+                       double tol, double* out);
+int launch_restart(Ctx* c);
+int launch_power_A(Ctx* c, int maxit, double tol, double* lam);
+int launch_power_Q(Ctx* c, int maxit, double tol, double* lam);
+int push_state(Ctx* c);
+int update_q_factors(Ctx* c);
+int launch_unscale(Ctx* c, double* x, double* y, double* z, double* w);
+int launch_initial_points(Ctx* c, const double* x0, const double* y0);
+int repack_values(Ctx* c);
+double iteration_bytes(const Ctx* c);
+// scaling (hpr_scale.cu)
+int run_scaling(Ctx* c, const hpr_params* p, hpr_scale_info* out);
+
+// host-side start vector for the power iteration (splitmix64 uniform(-1,1)
+// + 1e-8).  The reference uses randn(MersenneTwister(1)) .+ 1e-8
+// (src/utils/eigenvalues.jl:72-76), which has no portable equivalent.
+void power_start_vector(std::vector<double>& z, uint64_t seed);
+
+}  // namespace hpr
+
+struct hpr_ctx {
+  hpr::Ctx c;
+};

@@ -1,0 +1,1157 @@
+// hpr_kernels.cu — epilogues of the fused engine and their launchers: the HPR
+// half-steps, residuals, M-norm, sigma terms, restarts, power iteration and
+// unscaling.  Arithmetic follows the reference's operation order (file:line
+// beside each epilogue); the library is compiled with -fmad=false so the only
+// fused multiply-adds are the explicit fma() calls standing for the
+// reference's `muladd`.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "hpr_engine.cuh"
+
+namespace hpr {
+
+// ---------------------------------------------------------------------------
+// Halpern factors from the device-resident counter
+// (main_update_gpu!, algorithm.jl:2287-2289).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void halpern(const DevState* st, double& H1, double& H2) {
+  long long in = *((volatile const long long*)&st->inner);
+  H1 = 1.0 / ((double)in + 2.0);
+  H2 = 1.0 - H1;
+}
+
+// ---------------------------------------------------------------------------
+// x half-step without Q: unified_update_zx_kernel_full!/partial!
+// (kernels.jl:5955-6063) and the SOC variable projections (kernels.jl:
+// 1652-1706); CPU twin unified_update_zx_cpu! (kernels.jl:7672-7812).
+// ---------------------------------------------------------------------------
+struct EpiX {
+  static constexpr bool kCones = true;
+  static constexpr int kNRed = 0;
+  static constexpr unsigned kMaxMask = 0;
+  const double *c, *l, *u, *last_x;
+  double *x, *x_hat, *x_bar, *z_bar, *dx;
+  float* x_hat32;
+  int full;
+  double sigma, H1, H2;
+  __device__ void setup(const DevState* st) {
+    sigma = st->sigma;
+    halpern(st, H1, H2);
+  }
+  __device__ __forceinline__ void finish(int64_t i, double xi, double xb, double zr) {
+    double xh = 2.0 * xb - xi;
+    double xn = fma(H2, xh, H1 * last_x[i]);
+    if (full) {
+      dx[i] = xb - xi;
+      x_bar[i] = xb;
+      z_bar[i] = (xb - zr) / sigma;
+    }
+    x[i] = xn;
+    x_hat[i] = xh;
+    if (x_hat32) x_hat32[i] = (float)xh;
+  }
+  __device__ void linear(int64_t i, double aty, Red&) {
+    double xi = x[i];
+    double tmp = aty - c[i];
+    double zr = xi + sigma * tmp;
+    double xb = cmin(cmax(zr, l[i]), u[i]);
+    finish(i, xi, xb, zr);
+  }
+  __device__ double cone_raw(int64_t i, double aty, Red&) { return x[i] + sigma * (aty - c[i]); }
+  __device__ void cone_apply(int64_t i, double zr, double t, double ns, bool head, Red&) {
+    double xb;
+    if (ns <= -t) xb = 0.0;
+    else if (ns <= t) xb = zr;
+    else {
+      double pt = (ns + t) / 2.0;
+      xb = head ? pt : (pt / ns) * zr;
+    }
+    finish(i, x[i], xb, zr);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// y half-step: unified_update_y_kernel_full!/partial! (kernels.jl:4354-4456)
+// and the SOC constraint projections (kernels.jl:4458-5368); CPU twins
+// unified_update_y_noQ_cpu! (7817-7952) and update_y_cpu! (7976-8096).
+// ---------------------------------------------------------------------------
+struct EpiY {
+  static constexpr bool kCones = true;
+  static constexpr int kNRed = 0;
+  static constexpr unsigned kMaxMask = 0;
+  const double *AL, *AU, *rhs, *last_y;
+  double *y, *y_bar, *s, *dy;
+  float* y32;
+  int64_t m_lin;
+  int full, ybar_always;
+  double f1, f2, H1, H2;
+  __device__ void setup(const DevState* st) {
+    f1 = st->lamA * st->sigma;
+    f2 = 1.0 / f1;
+    halpern(st, H1, H2);
+  }
+  __device__ __forceinline__ void finish(int64_t i, double yi, double yb, double sp) {
+    double yh = 2.0 * yb - yi;
+    double yn = fma(H2, yh, H1 * last_y[i]);
+    if (full) {
+      s[i] = sp;
+      dy[i] = yb - yi;
+      y_bar[i] = yb;
+    } else if (ybar_always) {
+      y_bar[i] = yb;
+    }
+    y[i] = yn;
+    if (y32) y32[i] = (float)yn;
+  }
+  __device__ void linear(int64_t i, double ax, Red&) {
+    double yi = y[i];
+    double sr = ax - f1 * yi;
+    double sp = cmin(cmax(sr, AL[i]), AU[i]);
+    double corr = sp - sr;
+    double yb = f2 * corr;
+    finish(i, yi, yb, sp);
+  }
+  __device__ double cone_raw(int64_t i, double ax, Red&) { return ax - rhs[i - m_lin] - f1 * y[i]; }
+  __device__ void cone_apply(int64_t i, double sr, double t, double ns, bool head, Red&) {
+    double sp;
+    if (ns <= -t) sp = 0.0;
+    else if (ns <= t) sp = sr;
+    else {
+      double pt = (ns + t) / 2.0;
+      sp = head ? pt : (pt / ns) * sr;
+    }
+    double yb = f2 * (sp - sr);
+    finish(i, y[i], yb, sp);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Q path, x/w half-step: unified_update_zxw1_kernel_full!/partial!
+// (kernels.jl:379-494) with the SOC-with-Q projections (634-1263); CPU twin
+// update_zxw1_cpu! (7487-7664).  qdiag != null means the operator
+// diag(qdiag) + F'F and `v` is (F'(F w))_i.
+// ---------------------------------------------------------------------------
+struct EpiQX {
+  static constexpr bool kCones = true;
+  static constexpr int kNRed = 0;
+  static constexpr unsigned kMaxMask = 0;
+  const double *c, *l, *u, *last_x, *aty, *w, *fact1, *fact2, *qdiag;
+  double *x, *x_hat, *x_bar, *z_bar, *dx, *w_bar, *Qw;
+  int full, diag;
+  double sigma, H1, H2, f1s, f2s;
+  __device__ void setup(const DevState* st) {
+    sigma = st->sigma;
+    halpern(st, H1, H2);
+    f2s = 1.0 / (1.0 + st->sigma * st->lamQ);
+    f1s = 1.0 - f2s;
+  }
+  __device__ __forceinline__ double qw(int64_t i, double v) { return qdiag ? qdiag[i] * w[i] + v : v; }
+  __device__ __forceinline__ void finish(int64_t i, double xi, double xb, double zr) {
+    double xh = 2.0 * xb - xi;
+    double xn = fma(H2, xh, H1 * last_x[i]);
+    w_bar[i] = diag ? fma(fact1[i], w[i], fact2[i] * xh) : fma(f1s, w[i], f2s * xh);
+    if (full) {
+      dx[i] = xb - xi;
+      x_bar[i] = xb;
+      z_bar[i] = (xb - zr) / sigma;
+    }
+    x[i] = xn;
+    x_hat[i] = xh;
+  }
+  __device__ void linear(int64_t i, double v, Red&) {
+    double q = qw(i, v);
+    Qw[i] = q;
+    double xi = x[i];
+    double tmp = -q + aty[i] - c[i];
+    double zr = xi + sigma * tmp;
+    double xb = cmin(cmax(zr, l[i]), u[i]);
+    finish(i, xi, xb, zr);
+  }
+  __device__ double cone_raw(int64_t i, double v, Red&) {
+    double q = qw(i, v);
+    Qw[i] = q;
+    return x[i] + sigma * (-q + aty[i] - c[i]);
+  }
+  __device__ void cone_apply(int64_t i, double zr, double t, double ns, bool head, Red&) {
+    double xb;
+    if (ns <= -t) xb = 0.0;
+    else if (ns <= t) xb = zr;
+    else {
+      double pt = (ns + t) / 2.0;
+      xb = head ? pt : (pt / ns) * zr;
+    }
+    finish(i, x[i], xb, zr);
+  }
+};
+
+// tempv = x_hat + sigma (Qw - Q w_bar): compute_tempv_unified_kernel!
+// (kernels.jl:4268-4299); CPU update_y_cpu! (kernels.jl:7988-7989).
+struct EpiQT {
+  static constexpr bool kCones = false;
+  static constexpr int kNRed = 0;
+  static constexpr unsigned kMaxMask = 0;
+  const double *x_hat, *Qw, *w_bar, *qdiag;
+  double* tempv;
+  float* tempv32;
+  double sigma;
+  __device__ void setup(const DevState* st) { sigma = st->sigma; }
+  __device__ void linear(int64_t i, double v, Red&) {
+    double qwb = qdiag ? qdiag[i] * w_bar[i] + v : v;
+    double tv = x_hat[i] + sigma * (Qw[i] - qwb);
+    tempv[i] = tv;
+    if (tempv32) tempv32[i] = (float)tv;
+  }
+  __device__ double cone_raw(int64_t, double v, Red&) { return v; }
+  __device__ void cone_apply(int64_t, double, double, double, bool, Red&) {}
+};
+
+// w2 half-step: unified_update_w2_kernel_full!/partial! (kernels.jl:
+// 5384-5497); CPU update_w2_cpu! (kernels.jl:8100-8185).
+struct EpiW2 {
+  static constexpr bool kCones = false;
+  static constexpr int kNRed = 0;
+  static constexpr unsigned kMaxMask = 0;
+  const double *last_w, *last_aty, *fact;
+  double *w, *w_bar, *aty, *aty_bar, *dw, *atdy;
+  int full, diag;
+  double H1, H2, fs;
+  __device__ void setup(const DevState* st) {
+    halpern(st, H1, H2);
+    fs = st->sigma / (1.0 + st->sigma * st->lamQ);
+  }
+  __device__ void linear(int64_t i, double ab, Red&) {
+    double wi = w[i], wbi = w_bar[i], ai = aty[i];
+    double f = diag ? fact[i] : fs;
+    double wbn = wbi + f * (ab - ai);
+    double wn = H1 * last_w[i] + H2 * (2.0 * wbn - wi);
+    double an = H1 * last_aty[i] + H2 * (2.0 * ab - ai);
+    w[i] = wn;
+    aty[i] = an;
+    if (full) {
+      w_bar[i] = wbn;
+      dw[i] = wbn - wi;
+      atdy[i] = ab - ai;
+      aty_bar[i] = ab;
+    }
+  }
+  __device__ double cone_raw(int64_t, double v, Red&) { return v; }
+  __device__ void cone_apply(int64_t, double, double, double, bool, Red&) {}
+};
+
+// out = M v (+ diag(qdiag) vin for the diag + F'F operator).
+struct EpiPlain {
+  static constexpr bool kCones = false;
+  static constexpr int kNRed = 0;
+  static constexpr unsigned kMaxMask = 0;
+  double* out;
+  const double *qdiag, *vin;
+  __device__ void setup(const DevState*) {}
+  __device__ void linear(int64_t i, double v, Red&) { out[i] = qdiag ? qdiag[i] * vin[i] + v : v; }
+  __device__ double cone_raw(int64_t, double v, Red&) { return v; }
+  __device__ void cone_apply(int64_t, double, double, double, bool, Red&) {}
+};
+
+// out = M v and <out, other>.
+struct EpiDot {
+  static constexpr bool kCones = false;
+  static constexpr int kNRed = 1;
+  static constexpr unsigned kMaxMask = 0;
+  double* out;
+  const double* other;
+  __device__ void setup(const DevState*) {}
+  __device__ void linear(int64_t i, double v, Red& r) {
+    out[i] = v;
+    r.v[0] = r.v[0] + v * other[i];
+  }
+  __device__ double cone_raw(int64_t, double v, Red&) { return v; }
+  __device__ void cone_apply(int64_t, double, double, double, bool, Red&) {}
+};
+
+// Dual residual in original coordinates: compute_Rd_kernel! /
+// compute_Rd_noQ_kernel! (kernels.jl:6467-6512) with the objective dots of
+// compute_residuals! (algorithm.jl:113-160).
+// lanes: 0 max|Rd|, 1 max|A'y_org|, 2 max|Qx_org|, 3 c'x, 4 z'x, 5 x'Qx
+struct EpiRd {
+  static constexpr bool kCones = false;
+  static constexpr int kNRed = 6;
+  static constexpr unsigned kMaxMask = 0x7;
+  const double *c, *z_bar, *x_bar, *col_norm, *Qx;
+  double cs;
+  __device__ void setup(const DevState*) {}
+  __device__ void linear(int64_t i, double v, Red& r) {
+    double cn = col_norm[i];
+    double c_org = c[i] * cn * cs;
+    double a_org = v * cn * cs;
+    double z_org = z_bar[i] * cn * cs;
+    double rd;
+    if (Qx) {
+      double q_org = Qx[i] * cn * cs;
+      rd = q_org + c_org - a_org - z_org;
+      r.v[2] = nanmax(r.v[2], fabs(q_org));
+      r.v[5] = r.v[5] + x_bar[i] * Qx[i];
+    } else {
+      rd = c_org - a_org - z_org;
+    }
+    r.v[0] = nanmax(r.v[0], fabs(rd));
+    r.v[1] = nanmax(r.v[1], fabs(a_org));
+    r.v[3] = r.v[3] + c[i] * x_bar[i];
+    r.v[4] = r.v[4] + z_bar[i] * x_bar[i];
+  }
+  __device__ double cone_raw(int64_t, double v, Red&) { return v; }
+  __device__ void cone_apply(int64_t, double, double, double, bool, Red&) {}
+};
+
+// Primal residual in original coordinates: compute_Rp_kernel! and
+// compute_Rp_SOC_kernel! (kernels.jl:6523-6585) with the dual-objective dots
+// y's and y'soc_rhs (algorithm.jl:150-153).
+// lanes: 0 max|Rp_lin|, 1 max|Rp_soc|, 2 max|Ax_org|, 3 y's, 4 y'rhs
+struct EpiRp {
+  static constexpr bool kCones = true;
+  static constexpr int kNRed = 5;
+  static constexpr unsigned kMaxMask = 0x7;
+  const double *AL, *AU, *rhs, *rhs_full, *row_norm, *y_bar, *s;
+  int64_t m_lin;
+  double bs;
+  __device__ void setup(const DevState*) {}
+  __device__ void linear(int64_t i, double v, Red& r) {
+    double rn = row_norm[i];
+    double ax = v * rn * bs;
+    double lo = AL[i] * rn * bs;
+    double hi = AU[i] * rn * bs;
+    double pr = cmin(cmax(ax, lo), hi);
+    double rp = pr - ax;
+    r.v[0] = nanmax(r.v[0], fabs(rp));
+    r.v[2] = nanmax(r.v[2], fabs(ax));
+    r.v[3] = r.v[3] + y_bar[i] * s[i];
+    r.v[4] = r.v[4] + y_bar[i] * rhs_full[i];
+  }
+  __device__ double cone_raw(int64_t i, double v, Red& r) {
+    double rn = row_norm[i];
+    double ax = v * rn * bs;
+    double rt = rhs[i - m_lin] * rn * bs;
+    r.v[2] = nanmax(r.v[2], fabs(ax));
+    r.v[3] = r.v[3] + y_bar[i] * s[i];
+    r.v[4] = r.v[4] + y_bar[i] * rhs_full[i];
+    return ax - rt;
+  }
+  __device__ void cone_apply(int64_t i, double sr, double t, double ns, bool head, Red& r) {
+    double rp;
+    if (ns <= -t) rp = sr;
+    else if (ns <= t) rp = 0.0;
+    else if (head) rp = (ns + t) / 2 - t;
+    else {
+      double f = (1 + t / ns) / 2;
+      rp = f * sr - sr;
+    }
+    r.v[1] = nanmax(r.v[1], fabs(rp));
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Small kernels
+// ---------------------------------------------------------------------------
+__global__ void bump_inner_kernel(DevState* st) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) st->inner = st->inner + 1;
+}
+
+// ---------------------------------------------------------------------------
+// Host helpers
+// ---------------------------------------------------------------------------
+int upload_plan(Ctx* c, Plan& p) {
+  int64_t nt = (int64_t)p.tasks.size();
+  HPR_TRY(dev_alloc_n(c, &p.d_tasks, nt));
+  HPR_TRY(dev_alloc_n(c, &p.d_big, (int64_t)p.big.size()));
+  HPR_TRY(dev_alloc_n(c, &p.d_lng, (int64_t)p.lng.size()));
+  HPR_TRY(dev_alloc_n(c, &p.d_big_cnt, (int64_t)p.big.size()));
+  HPR_TRY(dev_alloc_n(c, &p.d_lng_cnt, (int64_t)p.lng.size()));
+  HPR_TRY(dev_alloc_n(c, &p.d_partials, (int64_t)p.npartials));
+  HPR_TRY(dev_alloc_n(c, &p.d_raw, p.nrows));
+  if (nt) HPR_CUDA(c, cudaMemcpy(p.d_tasks, p.tasks.data(), nt * sizeof(Task), cudaMemcpyHostToDevice));
+  if (!p.big.empty())
+    HPR_CUDA(c, cudaMemcpy(p.d_big, p.big.data(), p.big.size() * sizeof(BigCone), cudaMemcpyHostToDevice));
+  if (!p.lng.empty())
+    HPR_CUDA(c, cudaMemcpy(p.d_lng, p.lng.data(), p.lng.size() * sizeof(LongRow), cudaMemcpyHostToDevice));
+  HPR_CUDA(c, cudaMemset(p.d_big_cnt, 0, std::max<size_t>(1, p.big.size()) * sizeof(int32_t)));
+  HPR_CUDA(c, cudaMemset(p.d_lng_cnt, 0, std::max<size_t>(1, p.lng.size()) * sizeof(int32_t)));
+  int64_t need = (int64_t)p.nslots() * kMaxRed;
+  if (need > c->red_slots) {
+    if (c->d_red) {
+      cudaFree(c->d_red);
+      c->used -= (size_t)c->red_slots * sizeof(double);
+    }
+    c->red_slots = 0;
+    HPR_TRY(dev_alloc_n(c, &c->d_red, need));
+    c->red_slots = need;
+  }
+  return HPR_OK;
+}
+
+PlanView view_of(const Plan& p, const int32_t* cone_start) {
+  PlanView v;
+  v.tasks = p.d_tasks;
+  v.big = p.d_big;
+  v.lng = p.d_lng;
+  v.big_cnt = p.d_big_cnt;
+  v.lng_cnt = p.d_lng_cnt;
+  v.partials = p.d_partials;
+  v.raw = p.d_raw;
+  v.cone_start = cone_start;
+  v.ntasks = (int32_t)p.tasks.size();
+  v.nbig = (int32_t)p.big.size();
+  v.nlng = (int32_t)p.lng.size();
+  return v;
+}
+
+namespace {
+
+template <class Epi>
+int engine_launch(Ctx* c, const DevCSR& M, const Plan& p, const int32_t* cone_start, const double* xin,
+                  const float* xin32, const Epi& epi, bool bump, bool with_red, int red_off) {
+  int nt = (int)p.tasks.size();
+  if (nt == 0) {
+    if (bump) bump_inner_kernel<<<1, 32, 0, c->stream>>>(c->d_state);
+    if (with_red) {
+      // no rows: reductions are the identity
+      HPR_CUDA(c, cudaMemsetAsync(c->d_red_out + red_off, 0, Epi::kNRed * sizeof(double), c->stream));
+    }
+    return HPR_OK;
+  }
+  EngineArgs a;
+  a.M = M;
+  a.xin = xin;
+  a.xin32 = xin32;
+  a.pv = view_of(p, cone_start);
+  a.st = c->d_state;
+  a.red_slots = with_red ? c->d_red : nullptr;
+  a.bump_inner = bump ? 1 : 0;
+  if (c->precision == HPR_PREC_FP32 && xin32 && M.val32)
+    engine_kernel<Epi, HPR_PREC_FP32><<<nt, kThreads, 0, c->stream>>>(a, epi);
+  else if (c->precision == HPR_PREC_BF16 && xin32 && M.val16)
+    engine_kernel<Epi, HPR_PREC_BF16><<<nt, kThreads, 0, c->stream>>>(a, epi);
+  else
+    engine_kernel<Epi, HPR_PREC_FP64><<<nt, kThreads, 0, c->stream>>>(a, epi);
+  c->launches++;
+  HPR_CUDA(c, cudaGetLastError());
+  if (with_red) {
+    final_reduce_kernel<Epi::kNRed, Epi::kMaxMask><<<1, kThreads, 0, c->stream>>>(c->d_red, p.nslots(),
+                                                                                   c->d_red_out + red_off);
+    c->launches++;
+    HPR_CUDA(c, cudaGetLastError());
+  }
+  return HPR_OK;
+}
+
+// Q v into out (Qmap!, sparse_matrix_operator.jl:27-51); tmp holds F v for
+// the diag + F'F operator.
+int qmap(Ctx* c, const double* v, double* out, double* tmp) {
+  if (c->q_kind == HPR_Q_CSR) {
+    EpiPlain e{out, nullptr, nullptr};
+    return engine_launch(c, c->Q, c->planQ, c->d_var_start, v, nullptr, e, false, false, 0);
+  }
+  if (c->q_kind == HPR_Q_DIAG_LOWRANK) {
+    EpiPlain e1{tmp, nullptr, nullptr};
+    HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, v, nullptr, e1, false, false, 0));
+    EpiPlain e2{out, c->qdiag, v};
+    return engine_launch(c, c->FT, c->planQ, c->d_var_start, tmp, nullptr, e2, false, false, 0);
+  }
+  HPR_CUDA(c, cudaMemsetAsync(out, 0, c->n * sizeof(double), c->stream));
+  return HPR_OK;
+}
+
+struct DotF {
+  const double *a, *b;
+  __device__ void operator()(int64_t i, Red& r) const { r.v[0] = r.v[0] + a[i] * b[i]; }
+};
+struct Dot2F {
+  const double *a, *b, *c, *d;
+  __device__ void operator()(int64_t i, Red& r) const {
+    r.v[0] = r.v[0] + a[i] * b[i];
+    r.v[1] = r.v[1] + c[i] * d[i];
+  }
+};
+struct AbsMaxF {
+  const double* a;
+  __device__ void operator()(int64_t i, Red& r) const { r.v[0] = nanmax(r.v[0], fabs(a[i])); }
+};
+
+int dot(Ctx* c, int64_t n, const double* a, const double* b, double* out) {
+  HPR_TRY(vec_reduce<1, 0>(c, n, DotF{a, b}, 0));
+  HPR_TRY(fetch_red(c, 1));
+  *out = c->h_red_out[0];
+  return HPR_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Iteration
+// ---------------------------------------------------------------------------
+int push_state(Ctx* c) {
+  c->h_state->sigma = c->sigma;
+  c->h_state->lamA = c->lamA;
+  c->h_state->lamQ = c->lamQ;
+  c->h_state->pad0 = 0;
+  c->h_state->inner = c->inner;
+  c->h_state->ticket = 0;
+  c->h_state->error = 0;
+  HPR_CUDA(c, cudaMemcpyAsync(c->d_state, c->h_state, sizeof(DevState), cudaMemcpyHostToDevice, c->stream));
+  // the staging buffer is reused: make the copy complete before returning
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  return HPR_OK;
+}
+
+int update_q_factors(Ctx* c) {
+  // unified_update_Q_factors! (unified_operations.jl:484-498)
+  if (!c->Q_is_diag || !c->has_q) return HPR_OK;
+  double s = c->sigma, s2 = s * s;
+  const double* dq = c->diag_Q;
+  double *f2 = c->fact2, *f = c->fact, *f1 = c->fact1, *fm = c->fact_M;
+  return vec_map(c, c->n, [=] __device__(int64_t i) {
+    double t2 = 1.0 / (1.0 + s * dq[i]);
+    f2[i] = t2;
+    f[i] = s * t2;
+    f1[i] = s * dq[i] * t2;
+    fm[i] = s2 * t2;
+  });
+}
+
+int launch_iteration(Ctx* c, bool full) {
+  const bool fp32 = c->precision != HPR_PREC_FP64;
+  if (!c->has_q) {
+    // main_update_noQ_soc_gpu! (algorithm.jl:2302-2309)
+    EpiX ex;
+    ex.c = c->c;
+    ex.l = c->l;
+    ex.u = c->u;
+    ex.last_x = c->last_x;
+    ex.x = c->x;
+    ex.x_hat = c->x_hat;
+    ex.x_bar = c->x_bar;
+    ex.z_bar = c->z_bar;
+    ex.dx = c->dx;
+    ex.x_hat32 = fp32 ? c->g32_n : nullptr;
+    ex.full = full ? 1 : 0;
+    HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y, fp32 ? c->g32_m : nullptr, ex,
+                          c->m == 0, false, 0));
+    if (c->m > 0) {
+      EpiY ey;
+      ey.AL = c->AL;
+      ey.AU = c->AU;
+      ey.rhs = c->soc_rhs;
+      ey.last_y = c->last_y;
+      ey.y = c->y;
+      ey.y_bar = c->y_bar;
+      ey.s = c->s;
+      ey.dy = c->dy;
+      ey.y32 = fp32 ? c->g32_m : nullptr;
+      ey.m_lin = c->m_lin;
+      ey.full = full ? 1 : 0;
+      ey.ybar_always = 0;
+      HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->x_hat, fp32 ? c->g32_n : nullptr,
+                            ey, true, false, 0));
+    }
+    return HPR_OK;
+  }
+  // Q path: zxw1, y, w2 (algorithm.jl:2291-2295)
+  const bool lowrank = c->q_kind == HPR_Q_DIAG_LOWRANK;
+  EpiQX eq;
+  eq.c = c->c;
+  eq.l = c->l;
+  eq.u = c->u;
+  eq.last_x = c->last_x;
+  eq.aty = c->ATy;
+  eq.w = c->w;
+  eq.fact1 = c->fact1;
+  eq.fact2 = c->fact2;
+  eq.qdiag = lowrank ? c->qdiag : nullptr;
+  eq.x = c->x;
+  eq.x_hat = c->x_hat;
+  eq.x_bar = c->x_bar;
+  eq.z_bar = c->z_bar;
+  eq.dx = c->dx;
+  eq.w_bar = c->w_bar;
+  eq.Qw = c->Qw;
+  eq.full = full ? 1 : 0;
+  eq.diag = c->Q_is_diag ? 1 : 0;
+  if (lowrank) {
+    EpiPlain ef{c->ftmp, nullptr, nullptr};
+    HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, c->w, nullptr, ef, false, false, 0));
+    HPR_TRY(engine_launch(c, c->FT, c->planQ, c->d_var_start, c->ftmp, nullptr, eq, false, false, 0));
+  } else {
+    HPR_TRY(engine_launch(c, c->Q, c->planQ, c->d_var_start, c->w, nullptr, eq, false, false, 0));
+  }
+  if (c->m > 0) {
+    EpiQT et;
+    et.x_hat = c->x_hat;
+    et.Qw = c->Qw;
+    et.w_bar = c->w_bar;
+    et.qdiag = lowrank ? c->qdiag : nullptr;
+    et.tempv = c->tempv;
+    et.tempv32 = fp32 ? c->g32_n : nullptr;
+    if (lowrank) {
+      EpiPlain ef{c->ftmp2, nullptr, nullptr};
+      HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, c->w_bar, nullptr, ef, false, false, 0));
+      HPR_TRY(engine_launch(c, c->FT, c->planQ, c->d_var_start, c->ftmp2, nullptr, et, false, false, 0));
+    } else {
+      HPR_TRY(engine_launch(c, c->Q, c->planQ, c->d_var_start, c->w_bar, nullptr, et, false, false, 0));
+    }
+    EpiY ey;
+    ey.AL = c->AL;
+    ey.AU = c->AU;
+    ey.rhs = c->soc_rhs;
+    ey.last_y = c->last_y;
+    ey.y = c->y;
+    ey.y_bar = c->y_bar;
+    ey.s = c->s;
+    ey.dy = c->dy;
+    ey.y32 = fp32 ? c->g32_m : nullptr;
+    ey.m_lin = c->m_lin;
+    ey.full = full ? 1 : 0;
+    ey.ybar_always = 1;
+    HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->tempv, fp32 ? c->g32_n : nullptr, ey,
+                          false, false, 0));
+  }
+  EpiW2 e2;
+  e2.last_w = c->last_w;
+  e2.last_aty = c->last_ATy;
+  e2.fact = c->fact;
+  e2.w = c->w;
+  e2.w_bar = c->w_bar;
+  e2.aty = c->ATy;
+  e2.aty_bar = c->ATy_bar;
+  e2.dw = c->dw;
+  e2.atdy = c->ATdy;
+  e2.full = full ? 1 : 0;
+  e2.diag = c->Q_is_diag ? 1 : 0;
+  return engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, e2,
+                       true, false, 0);
+}
+
+int run_iterations(Ctx* c, int64_t k, bool full_last) {
+  if (k <= 0) return HPR_OK;
+  int64_t l0 = c->launches;
+  HPR_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+  int64_t partial = full_last ? k - 1 : k;
+  int64_t done = 0;
+  // replay the captured partial-iteration graph where it fits
+  if (c->graph_partial && c->graph_iters > 0) {
+    while (partial - done >= c->graph_iters) {
+      HPR_CUDA(c, cudaGraphLaunch(c->graph_partial, c->stream));
+      done += c->graph_iters;
+      c->launches += c->graph_iters * (c->has_q ? 4 : 2);
+    }
+  }
+  for (; done < partial; ++done) HPR_TRY(launch_iteration(c, false));
+  if (full_last) HPR_TRY(launch_iteration(c, true));
+  HPR_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+  c->inner += k;
+  c->last_launches = c->launches - l0;
+  return HPR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Residuals (compute_residuals!, algorithm.jl:113-196)
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void bounds_box_kernel(int64_t n, const double* l, const double* u, const double* xb, const double* col,
+                                  double bs, double* dx) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double lv = cmax(l[i] - xb[i], 0.0);
+    double uv = cmax(xb[i] - u[i], 0.0);
+    dx[i] = (lv + uv) * (bs / col[i]);
+  }
+}
+// compute_err_soc_kernel! (kernels.jl:6617-6655)
+__global__ void bounds_cone_kernel(int64_t ncones, const int32_t* vs, const double* xb, const double* col, double bs,
+                                   double* dx) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < ncones; k += (int64_t)gridDim.x * blockDim.x) {
+    int64_t st = vs[k], en = vs[k + 1];
+    double t = xb[st];
+    double ns = 0.0;
+    dx[st] = t;
+    for (int64_t j = st + 1; j < en; ++j) {
+      dx[j] = xb[j];
+      ns += xb[j] * xb[j];
+    }
+    ns = sqrt(ns);
+    if (ns <= -t) {
+    } else if (ns <= t) {
+      for (int64_t j = st; j < en; ++j) dx[j] = 0.0;
+    } else {
+      double f = (1 + t / ns) / 2;
+      dx[st] = (ns + t) / 2 - t;
+      for (int64_t j = st + 1; j < en; ++j) dx[j] = f * dx[j] - dx[j];
+    }
+    for (int64_t j = st; j < en; ++j) dx[j] *= bs / col[j];
+  }
+}
+}  // namespace
+
+int launch_residuals(Ctx* c, bool include_bounds, hpr_residuals* r) {
+  const double bs = c->b_scale, cs = c->c_scale;
+  const bool skipq = !c->has_q;
+  // offsets in d_red_out: [0..5] Rd lanes, [8..12] Rp lanes, [16] bounds
+  if (!skipq) HPR_TRY(qmap(c, c->x_bar, c->Qx, c->ftmp));
+  EpiRd ed;
+  ed.c = c->c;
+  ed.z_bar = c->z_bar;
+  ed.x_bar = c->x_bar;
+  ed.col_norm = c->col_norm;
+  ed.Qx = skipq ? nullptr : c->Qx;
+  ed.cs = cs;
+  HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, ed, false, true, 0));
+  if (c->m > 0) {
+    EpiRp ep;
+    ep.AL = c->AL;
+    ep.AU = c->AU;
+    ep.rhs = c->soc_rhs;
+    ep.rhs_full = c->soc_rhs_full;
+    ep.row_norm = c->row_norm;
+    ep.y_bar = c->y_bar;
+    ep.s = c->s;
+    ep.m_lin = c->m_lin;
+    ep.bs = bs;
+    HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->x_bar, nullptr, ep, false, true, 8));
+  }
+  if (include_bounds) {
+    bounds_box_kernel<<<592, kThreads, 0, c->stream>>>(c->n, c->l, c->u, c->x_bar, c->col_norm, bs, c->dx);
+    int64_t nv = (int64_t)c->h_var_idx.size() - 1;
+    if (nv > 0)
+      bounds_cone_kernel<<<(int)std::min<int64_t>((nv + 127) / 128, 1184), 128, 0, c->stream>>>(
+          nv, c->d_var_start, c->x_bar, c->col_norm, bs, c->dx);
+    HPR_CUDA(c, cudaGetLastError());
+    HPR_TRY(vec_reduce<1, 1>(c, c->n, AbsMaxF{c->dx}, 16));
+  }
+  HPR_TRY(fetch_red(c, 17));
+  const double* h = c->h_red_out;
+  auto jmax = [](double a, double b) { return (a != a) ? a : ((b != b) ? b : (a > b ? a : b)); };
+  double qx_dot = skipq ? 0.0 : h[5];
+  r->primal_obj_bar = bs * cs * (h[3] + 0.5 * qx_dot) + c->obj_constant;
+  r->dual_obj_bar = bs * cs * (-0.5 * qx_dot + h[4]) + c->obj_constant;
+  if (c->m > 0) r->dual_obj_bar += bs * cs * (h[11] + h[12]);
+  r->rel_gap_bar = std::fabs(r->primal_obj_bar - r->dual_obj_bar) /
+                   (1.0 + std::max(std::fabs(r->primal_obj_bar), std::fabs(r->dual_obj_bar)));
+  double qx_inf = skipq ? 0.0 : h[2];
+  r->err_Rd_org_bar = h[0] / (1.0 + jmax(jmax(c->norm_c_org, h[1]), qx_inf));
+  if (c->m > 0) {
+    double denom = 1.0 + jmax(c->norm_b_org, h[10]);
+    double lin = c->m_lin > 0 ? h[8] / denom : 0.0;
+    double soc = c->m_lin < c->m ? h[9] / denom : 0.0;
+    r->err_Rp_linear_org_bar = lin;
+    r->err_Rp_soc_org_bar = soc;
+    r->err_Rp_org_bar = jmax(h[8], h[9]) / denom;
+  } else {
+    r->err_Rp_org_bar = r->err_Rp_linear_org_bar = r->err_Rp_soc_org_bar = 0.0;
+  }
+  if (include_bounds) r->err_Rp_org_bar = jmax(r->err_Rp_org_bar, h[16]);
+  r->KKTx_and_gap_org_bar = jmax(jmax(r->err_Rp_org_bar, r->err_Rd_org_bar), r->rel_gap_bar);
+  return HPR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// M-norm (compute_M_norm!, algorithm.jl:1302-1359)
+// ---------------------------------------------------------------------------
+int launch_mnorm(Ctx* c, double* out) {
+  const double sg = c->sigma;
+  const bool skipq = !c->has_q;
+  // [0] dx'dx, [1] dy'dy, [2] <A'dy, dx>, [3] dQw'dx, [4] dQw'ATdy,
+  // [5] ATdy'QATdy (diag: scaled by fact_M), [6] dQw'dQw, [7] dw'dQw
+  double h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  HPR_TRY(vec_reduce<1, 0>(c, c->n, DotF{c->dx, c->dx}, 0));
+  if (c->m > 0) HPR_TRY(vec_reduce<1, 0>(c, c->m, DotF{c->dy, c->dy}, 1));
+  if (!skipq) {
+    HPR_TRY(qmap(c, c->dw, c->dQw, c->ftmp));
+    HPR_TRY(vec_reduce<2, 0>(c, c->n, Dot2F{c->dQw, c->dx, c->dQw, c->dQw}, 3));  // [3], [4]=dQw'dQw tmp
+  }
+  if (c->m > 0) {
+    EpiDot e{c->ATdy, c->dx};
+    HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->dy, nullptr, e, false, true, 2));
+  }
+  HPR_TRY(fetch_red(c, 8));
+  for (int k = 0; k < 5; ++k) h[k] = c->h_red_out[k];
+  double dqw2 = h[4];
+  double M1 = 0.0, M2 = (1.0 / sg) * h[0], M3 = 0.0;
+  if (!skipq) M2 -= 2.0 * h[3];
+  if (c->m > 0) {
+    M1 = sg * c->lamA * h[1];
+    if (!skipq) {
+      HPR_TRY(qmap(c, c->ATdy, c->QATdy, c->ftmp));
+      const double* fm = c->fact_M;
+      double* atdy = c->ATdy;
+      bool dg = c->Q_is_diag;
+      HPR_TRY(vec_reduce<1, 0>(c, c->n, DotF{c->dQw, c->ATdy}, 0));
+      HPR_TRY(fetch_red(c, 1));
+      M1 -= 2.0 * sg * c->h_red_out[0];
+      M2 += 2.0 * h[2];
+      if (dg) HPR_TRY(vec_map(c, c->n, [=] __device__(int64_t i) { atdy[i] *= fm[i]; }));
+      HPR_TRY(vec_reduce<2, 0>(c, c->n, Dot2F{c->ATdy, c->QATdy, c->dw, c->dQw}, 0));
+      HPR_TRY(fetch_red(c, 2));
+      if (dg) {
+        M3 = c->h_red_out[0];
+        M1 += sg * dqw2;
+      } else {
+        M3 = (sg * sg) / (1.0 + sg * c->lamQ) * c->h_red_out[0];
+        M1 += sg * c->lamQ * c->h_red_out[1];
+      }
+    } else {
+      M2 += 2.0 * h[2];
+    }
+  } else if (!c->Q_is_diag && !skipq) {
+    HPR_TRY(vec_reduce<1, 0>(c, c->n, DotF{c->dw, c->dQw}, 0));
+    HPR_TRY(fetch_red(c, 1));
+    M1 = sg * c->lamQ * c->h_red_out[0];
+  }
+  M2 += std::max(M1, 0.0);
+  double M = std::max(M2, 0.0) + std::max(M3, 0.0);
+  *out = std::sqrt(M);
+  return HPR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// update_sigma! inner products (algorithm.jl:787-833)
+// ---------------------------------------------------------------------------
+namespace {
+struct DiffDotF {
+  const double *a, *b;
+  double* d;
+  __device__ void operator()(int64_t i, Red& r) const {
+    double v = a[i] - b[i];
+    d[i] = v;
+    r.v[0] = r.v[0] + v * v;
+  }
+};
+}  // namespace
+
+int launch_sigma_terms(Ctx* c, double* a, double* b, double* cc, double* d) {
+  const bool skipq = !c->has_q;
+  const int64_t n = c->n, m = c->m;
+  if (!skipq) {
+    const double *wb = c->w_bar, *lw = c->last_w;
+    double* dw = c->dw;
+    HPR_TRY(vec_map(c, n, [=] __device__(int64_t i) { dw[i] = wb[i] - lw[i]; }));
+    HPR_TRY(qmap(c, c->dw, c->dQw, c->ftmp));
+  }
+  HPR_TRY(vec_reduce<1, 0>(c, n, DiffDotF{c->x_bar, c->last_x, c->dx}, 0));
+  if (m > 0) HPR_TRY(vec_reduce<1, 0>(c, m, DiffDotF{c->y_bar, c->last_y, c->dy}, 1));
+  if (!skipq && m > 0) {
+    HPR_TRY(vec_reduce<1, 0>(c, n, DiffDotF{c->ATy_bar, c->last_ATy, c->ATdy}, 7));
+    HPR_TRY(qmap(c, c->ATdy, c->QATdy, c->ftmp));
+    HPR_TRY(vec_reduce<2, 0>(c, n, Dot2F{c->dQw, c->ATdy, c->ATdy, c->QATdy}, 2));
+  }
+  if (!skipq) HPR_TRY(vec_reduce<2, 0>(c, n, Dot2F{c->dQw, c->dQw, c->dw, c->dQw}, 4));
+  HPR_TRY(fetch_red(c, 8));
+  const double* h = c->h_red_out;
+  double A = 0.0, B = h[0], C = 0.0, D = 0.0;
+  if (m > 0) {
+    if (!skipq) A = c->lamA * h[1] - 2.0 * h[2];
+    else A = c->lamA * h[1];
+  }
+  if (!skipq) {
+    if (c->Q_is_diag) {
+      double nq = std::sqrt(h[4]);
+      A += nq * nq;
+    } else {
+      A += c->lamQ * h[5];
+      if (m > 0) {
+        C = h[3];
+        D = c->lamQ;
+      }
+    }
+  }
+  *a = A;
+  *b = B;
+  *cc = C;
+  *d = D;
+  return HPR_OK;
+}
+
+// unified_golden_Q_diag (unified_operations.jl:411-449): each evaluation is
+// one fused pass over diag(Q), A'dy and Q A'dy.
+namespace {
+struct GoldenF {
+  const double *dq, *c, *d;
+  double x;
+  __device__ void operator()(int64_t i, Red& r) const { r.v[0] = r.v[0] + c[i] * (d[i] / (1.0 + x * dq[i])); }
+};
+}  // namespace
+
+int launch_golden_diag(Ctx* c, double a, double b, double lo, double hi, double tol, double* out) {
+  const int maxiter = 200;
+  double phi = (std::sqrt(5.0) - 1.0) / 2.0;
+  auto f = [&](double x, double* fx) -> int {
+    HPR_TRY(vec_reduce<1, 0>(c, c->n, GoldenF{c->diag_Q, c->ATdy, c->QATdy, x}, 0));
+    HPR_TRY(fetch_red(c, 1));
+    *fx = a * x + b / x + x * x * c->h_red_out[0];
+    return HPR_OK;
+  };
+  double x1 = hi - phi * (hi - lo);
+  double x2 = lo + phi * (hi - lo);
+  double f1, f2;
+  HPR_TRY(f(x1, &f1));
+  HPR_TRY(f(x2, &f2));
+  int it = 0;
+  while (std::fabs(hi - lo) > tol * std::max(1.0, std::fabs(lo)) && it < maxiter) {
+    if (f1 > f2) {
+      lo = x1;
+      x1 = x2;
+      f1 = f2;
+      x2 = lo + phi * (hi - lo);
+      HPR_TRY(f(x2, &f2));
+    } else {
+      hi = x2;
+      x2 = x1;
+      f2 = f1;
+      x1 = hi - phi * (hi - lo);
+      HPR_TRY(f(x1, &f1));
+    }
+    it++;
+  }
+  *out = (f1 < f2) ? x1 : x2;
+  return HPR_OK;
+}
+
+// do_restart! (algorithm.jl:1130-1166)
+int launch_restart(Ctx* c) {
+  size_t nb = (size_t)c->n * sizeof(double), mb = (size_t)c->m * sizeof(double);
+  HPR_CUDA(c, cudaMemcpyAsync(c->x, c->x_bar, nb, cudaMemcpyDeviceToDevice, c->stream));
+  HPR_CUDA(c, cudaMemcpyAsync(c->last_x, c->x_bar, nb, cudaMemcpyDeviceToDevice, c->stream));
+  if (c->has_q) {
+    HPR_CUDA(c, cudaMemcpyAsync(c->w, c->w_bar, nb, cudaMemcpyDeviceToDevice, c->stream));
+    HPR_CUDA(c, cudaMemcpyAsync(c->last_w, c->w_bar, nb, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  if (c->m > 0) {
+    HPR_CUDA(c, cudaMemcpyAsync(c->y, c->y_bar, mb, cudaMemcpyDeviceToDevice, c->stream));
+    HPR_CUDA(c, cudaMemcpyAsync(c->last_y, c->y_bar, mb, cudaMemcpyDeviceToDevice, c->stream));
+    if (c->has_q) {
+      EpiPlain e{c->ATy_bar, nullptr, nullptr};
+      HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, e, false, false, 0));
+      HPR_CUDA(c, cudaMemcpyAsync(c->last_ATy, c->ATy_bar, nb, cudaMemcpyDeviceToDevice, c->stream));
+      HPR_CUDA(c, cudaMemcpyAsync(c->ATy, c->ATy_bar, nb, cudaMemcpyDeviceToDevice, c->stream));
+    }
+  }
+  if (c->precision != HPR_PREC_FP64 && c->m > 0) {
+    const double* y = c->y;
+    float* y32 = c->g32_m;
+    HPR_TRY(vec_map(c, c->m, [=] __device__(int64_t i) { y32[i] = (float)y[i]; }));
+  }
+  c->inner = 0;
+  return push_state(c);
+}
+
+// ---------------------------------------------------------------------------
+// Power iteration (power_iteration_A / _Q, eigenvalues.jl:68-196)
+// ---------------------------------------------------------------------------
+void power_start_vector(std::vector<double>& z, uint64_t seed) {
+  uint64_t s = seed;
+  for (size_t i = 0; i < z.size(); ++i) {
+    s += 0x9E3779B97F4A7C15ull;
+    uint64_t t = s;
+    t = (t ^ (t >> 30)) * 0xBF58476D1CE4E5B9ull;
+    t = (t ^ (t >> 27)) * 0x94D049BB133111EBull;
+    t ^= (t >> 31);
+    double u = (double)(t >> 11) * (1.0 / 9007199254740992.0);
+    z[i] = (2.0 * u - 1.0) + 1e-8;
+  }
+}
+
+namespace {
+int power_generic(Ctx* c, int64_t len, bool isA, int maxit, double tol, double* lam) {
+  std::vector<double> hz(len);
+  power_start_vector(hz, 1);
+  double *z = c->pz, *q = c->pq, *tq = c->ptq;
+  HPR_CUDA(c, cudaMemcpyAsync(z, hz.data(), len * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  double lambda = 1.0;
+  int rc = HPR_OK;
+  double* out = c->d_red_out;
+  for (int it = 0; it < maxit; ++it) {
+    // q = z / ||z||
+    if ((rc = vec_reduce<1, 0>(c, len, DotF{z, z}, 20)) != HPR_OK) break;
+    const double* nzp = out + 20;
+    if ((rc = vec_map(c, len, [=] __device__(int64_t i) { q[i] = z[i] / sqrt(*nzp); })) != HPR_OK) break;
+    if (isA) {
+      EpiPlain e1{tq, nullptr, nullptr};
+      if ((rc = engine_launch(c, c->AT, c->planX, c->d_var_start, q, nullptr, e1, false, false, 0)) != HPR_OK) break;
+      EpiPlain e2{z, nullptr, nullptr};
+      if ((rc = engine_launch(c, c->A, c->planY, c->d_con_start, tq, nullptr, e2, false, false, 0)) != HPR_OK) break;
+    } else {
+      if ((rc = qmap(c, q, z, c->ftmp)) != HPR_OK) break;
+    }
+    if ((rc = vec_reduce<1, 0>(c, len, DotF{q, z}, 21)) != HPR_OK) break;
+    const double* lp = out + 21;
+    if ((rc = vec_map(c, len, [=] __device__(int64_t i) { q[i] = z[i] - (*lp) * q[i]; })) != HPR_OK) break;
+    if ((rc = vec_reduce<2, 0>(c, len, Dot2F{q, q, z, z}, 22)) != HPR_OK) break;
+    if ((rc = fetch_red(c, 24)) != HPR_OK) break;
+    lambda = c->h_red_out[21];
+    double err = std::sqrt(c->h_red_out[22]) / (std::sqrt(c->h_red_out[23]) + lambda);
+    if (err < tol) break;
+  }
+  cudaStreamSynchronize(c->stream);
+  *lam = lambda;
+  return rc;
+}
+}  // namespace
+
+int launch_power_A(Ctx* c, int maxit, double tol, double* lam) {
+  if (c->m == 0) {
+    *lam = 0.0;
+    return HPR_OK;
+  }
+  return power_generic(c, c->m, true, maxit, tol, lam);
+}
+
+int launch_power_Q(Ctx* c, int maxit, double tol, double* lam) {
+  if (!c->has_q || c->n == 0) {
+    *lam = 0.0;
+    return HPR_OK;
+  }
+  return power_generic(c, c->n, false, maxit, tol, lam);
+}
+
+// collect_results! unscaling (algorithm.jl:95-102, 1222-1256)
+int launch_unscale(Ctx* c, double* hx, double* hy, double* hz, double* hw) {
+  const double bs = c->b_scale, cs = c->c_scale;
+  const double *xb = c->x_bar, *col = c->col_norm, *zb = c->z_bar, *wb = c->w_bar, *yb = c->y_bar,
+               *row = c->row_norm;
+  double* t = c->vtmp_n;
+  size_t nb = (size_t)c->n * sizeof(double);
+  if (hx || (hw && !c->has_q)) {
+    HPR_TRY(vec_map(c, c->n, [=] __device__(int64_t i) { t[i] = bs * (xb[i] / col[i]); }));
+    if (hx) HPR_CUDA(c, cudaMemcpyAsync(hx, t, nb, cudaMemcpyDeviceToHost, c->stream));
+    if (hw && !c->has_q) HPR_CUDA(c, cudaMemcpyAsync(hw, t, nb, cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  if (hw && c->has_q) {
+    HPR_TRY(vec_map(c, c->n, [=] __device__(int64_t i) { t[i] = bs * (wb[i] / col[i]); }));
+    HPR_CUDA(c, cudaMemcpyAsync(hw, t, nb, cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  if (hz) {
+    HPR_TRY(vec_map(c, c->n, [=] __device__(int64_t i) { t[i] = cs * (zb[i] * col[i]); }));
+    HPR_CUDA(c, cudaMemcpyAsync(hz, t, nb, cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  if (hy && c->m > 0) {
+    double* tm = c->vtmp_m;
+    HPR_TRY(vec_map(c, c->m, [=] __device__(int64_t i) { tm[i] = cs * (yb[i] / row[i]); }));
+    HPR_CUDA(c, cudaMemcpyAsync(hy, tm, (size_t)c->m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  return HPR_OK;
+}
+
+// process_initial_points! (algorithm.jl:2612-2677)
+int launch_initial_points(Ctx* c, const double* hx0, const double* hy0) {
+  const double bs = c->b_scale, cs = c->c_scale;
+  const int64_t n = c->n, m = c->m;
+  const bool hq = c->has_q;
+  if (hx0) {
+    HPR_CUDA(c, cudaMemcpyAsync(c->vtmp_n, hx0, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const double *t = c->vtmp_n, *col = c->col_norm;
+    double *x = c->x, *xb = c->x_bar, *lx = c->last_x, *w = c->w, *wb = c->w_bar, *lw = c->last_w;
+    HPR_TRY(vec_map(c, n, [=] __device__(int64_t i) {
+      double v = t[i] * col[i] / bs;
+      x[i] = v;
+      xb[i] = v;
+      lx[i] = v;
+      if (hq) {
+        w[i] = v;
+        wb[i] = v;
+        lw[i] = v;
+      }
+    }));
+  }
+  if (hy0) {
+    HPR_CUDA(c, cudaMemcpyAsync(c->vtmp_m, hy0, m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const double *t = c->vtmp_m, *row = c->row_norm;
+    double *y = c->y, *yb = c->y_bar, *ly = c->last_y;
+    HPR_TRY(vec_map(c, m, [=] __device__(int64_t i) {
+      double v = t[i];
+      v = v * row[i] / cs;
+      y[i] = v;
+      yb[i] = v;
+      ly[i] = v;
+    }));
+    if (m > 0) {
+      if (hq) {
+        EpiPlain e{c->ATy_bar, nullptr, nullptr};
+        HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, e, false, false, 0));
+        HPR_CUDA(c, cudaMemcpyAsync(c->ATy, c->ATy_bar, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        HPR_CUDA(c, cudaMemcpyAsync(c->last_ATy, c->ATy_bar, n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                    c->stream));
+      } else {
+        EpiPlain e{c->ATy, nullptr, nullptr};
+        HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, e, false, false, 0));
+      }
+    }
+    if (hq) HPR_TRY(qmap(c, c->x_bar, c->Qx, c->ftmp));
+    const double *xb = c->x_bar, *aty = hq ? c->ATy_bar : c->ATy, *qx = c->Qx, *cc = c->c;
+    double* zb = c->z_bar;
+    const double sg = c->sigma;
+    HPR_TRY(vec_map(c, n, [=] __device__(int64_t i) {
+      double tmp = hq ? (-qx[i] + aty[i] - cc[i]) : (aty[i] - cc[i]);
+      double zr = xb[i] + sg * tmp;
+      zb[i] = (xb[i] - zr) / sg;
+    }));
+    if (m > 0) {
+      EpiPlain e{c->Ax, nullptr, nullptr};
+      HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->x_bar, nullptr, e, false, false, 0));
+      const double *ax = c->Ax, *yy = c->y, *al = c->AL, *au = c->AU;
+      double* s = c->s;
+      const double f1 = c->lamA * c->sigma;
+      HPR_TRY(vec_map(c, m, [=] __device__(int64_t i) { s[i] = cmin(cmax(ax[i] - f1 * yy[i], al[i]), au[i]); }));
+    }
+  }
+  if (c->precision != HPR_PREC_FP64 && m > 0) {
+    const double* y = c->y;
+    float* y32 = c->g32_m;
+    HPR_TRY(vec_map(c, m, [=] __device__(int64_t i) { y32[i] = (float)y[i]; }));
+  }
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  return HPR_OK;
+}
+
+// FP32 / BF16 copies of the scaled A and A' values (hpr_set_precision).
+int repack_values(Ctx* c) {
+  for (DevCSR* M : {&c->A, &c->AT}) {
+    if (M->nnz == 0) continue;
+    if (!M->val32) HPR_TRY(dev_alloc_n(c, &M->val32, M->nnz));
+    if (!M->val16) HPR_TRY(dev_alloc_n(c, &M->val16, M->nnz));
+    const double* v = M->val;
+    float* v32 = M->val32;
+    __nv_bfloat16* v16 = M->val16;
+    HPR_TRY(vec_map(c, M->nnz, [=] __device__(int64_t i) {
+      v32[i] = (float)v[i];
+      v16[i] = __double2bfloat16(v[i]);
+    }));
+  }
+  // FP32 gather copies of y (vtmp_m) and x_hat (vtmp_n) are kept by the
+  // epilogues; seed them from the current iterates.
+  if (c->m > 0) {
+    const double* y = c->y;
+    float* y32 = c->g32_m;
+    HPR_TRY(vec_map(c, c->m, [=] __device__(int64_t i) { y32[i] = (float)y[i]; }));
+  }
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  return HPR_OK;
+}
+
+// Algorithmic bytes of one partial no-Q iteration (roofline numerator):
+//   sum over A, A' of nnz*(value + 4) + 4*(rows+1) + gathered vector once,
+//   plus the epilogue streams (x r/w, last_x, c, x_hat w; l, u on boxed
+//   variables; y r/w, last_y; AL, AU on linear rows; soc_rhs on cone rows).
+double iteration_bytes(const Ctx* c) {
+  double sv = c->precision == HPR_PREC_FP64 ? 8.0 : (c->precision == HPR_PREC_FP32 ? 4.0 : 2.0);
+  double sg = c->precision == HPR_PREC_FP64 ? 8.0 : 4.0;
+  double nnz = (double)c->A.nnz;
+  double m = (double)c->m, n = (double)c->n;
+  double nb = (double)(((int64_t)c->h_var_idx.size() > 1) ? c->n_box : c->n);
+  double b = 2.0 * nnz * (sv + 4.0) + 4.0 * (m + 1) + 4.0 * (n + 1) + sg * (m + n);
+  b += n * 40.0 + nb * 16.0;       // x r/w, last_x, c, x_hat w; l, u
+  b += m * 24.0 + (double)c->m_lin * 16.0 + (m - (double)c->m_lin) * 8.0;  // y r/w, last_y; AL, AU; rhs
+  if (c->precision != HPR_PREC_FP64) b += (n + m) * 4.0;  // FP32 copies written
+  return b;
+}
+
+}  // namespace hpr

@@ -1,0 +1,174 @@
+// hpr_plan.cpp — host planner of the fused SpMV + epilogue engine.
+//
+// Takes the place of the reference's SOC bucket planner (configure_soc_*_
+// projection_paths!, src/algorithm.jl:1914-2223), which sorts cones into
+// size buckets with one kernel family each.  Here every row of a matrix side
+// is covered by cone-aligned tiles of at most kNnzTile nonzeros and kRowCap
+// rows, so one launch handles linear rows and cones of every size:
+//   * TASK_ROWS       — consecutive linear rows, or consecutive whole cones of
+//                       at most kSmallConeMax rows, finished inside the CTA;
+//   * TASK_CONE_PART  — a slice of a larger cone; the CTA that completes the
+//                       last slice projects the whole cone;
+//   * TASK_LONG_PART  — a nonzero slice of a row longer than one tile; the CTA
+//                       that completes the last slice adds the partial sums in
+//                       slice order and finishes the row.
+// Multi-CTA work is listed first so it starts in the first wave.
+#include <algorithm>
+
+#include "hpr_internal.h"
+
+namespace hpr {
+
+namespace {
+
+void emit_long_row(const std::vector<int32_t>& rp, int32_t r, int32_t bigslot,
+                   int32_t cone, Plan& plan, std::vector<Task>& out) {
+  int32_t nzb = rp[r], nze = rp[r + 1];
+  int32_t nparts = (nze - nzb + kNnzTile - 1) / kNnzTile;
+  LongRow lr;
+  lr.row = r;
+  lr.nparts = nparts;
+  lr.partial_base = plan.npartials;
+  lr.bigcone = bigslot;
+  int32_t slot = (int32_t)plan.lng.size();
+  plan.lng.push_back(lr);
+  plan.npartials += nparts;
+  for (int32_t p = 0; p < nparts; ++p) {
+    Task t{};
+    t.rb = r;
+    t.re = r + 1;
+    t.nzb = nzb + p * kNnzTile;
+    t.nze = std::min(nze, t.nzb + kNnzTile);
+    t.kind = TASK_LONG_PART;
+    t.ncones = 0;
+    t.cone = cone;
+    t.group = slot;
+    t.part = p;
+    out.push_back(t);
+  }
+}
+
+}  // namespace
+
+void build_plan(const std::vector<int32_t>& rp, int64_t nrows,
+                const std::vector<int64_t>& cone_starts, Plan& plan) {
+  plan.nrows = nrows;
+  plan.tasks.clear();
+  plan.big.clear();
+  plan.lng.clear();
+  plan.npartials = 0;
+  std::vector<Task> multi;  // multi-CTA work, emitted first
+  std::vector<Task> rows;
+  const int64_t lin_end = cone_starts.empty() ? nrows : cone_starts[0];
+
+  // ---- linear rows
+  int64_t r = 0;
+  while (r < lin_end) {
+    int64_t start = r, cnt = 0, nz = 0;
+    while (r < lin_end && cnt < kRowCap) {
+      int64_t rn = (int64_t)rp[r + 1] - rp[r];
+      if (rn > kNnzTile) break;
+      if (nz + rn > kNnzTile && cnt > 0) break;
+      nz += rn;
+      cnt++;
+      r++;
+    }
+    if (cnt > 0) {
+      Task t{};
+      t.rb = (int32_t)start;
+      t.re = (int32_t)r;
+      t.nzb = rp[start];
+      t.nze = rp[r];
+      t.kind = TASK_ROWS;
+      t.ncones = 0;
+      t.cone = -1;
+      t.group = -1;
+      rows.push_back(t);
+    }
+    if (r < lin_end && (int64_t)rp[r + 1] - rp[r] > kNnzTile) {
+      emit_long_row(rp, (int32_t)r, -1, -1, plan, multi);
+      r++;
+    }
+  }
+
+  // ---- cones
+  int64_t ncones = cone_starts.empty() ? 0 : (int64_t)cone_starts.size() - 1;
+  Task cur{};
+  bool open = false;
+  auto flush = [&]() {
+    if (open) rows.push_back(cur);
+    open = false;
+  };
+  for (int64_t k = 0; k < ncones; ++k) {
+    int64_t a = cone_starts[k], b = cone_starts[k + 1];
+    int64_t d = b - a;
+    int64_t cnz = (int64_t)rp[b] - rp[a];
+    bool big = d > kSmallConeMax || cnz > kNnzTile;
+    if (d <= 0) continue;
+    if (!big) {
+      if (open && ((cur.re - cur.rb) + d > kRowCap ||
+                   (int64_t)(cur.nze - cur.nzb) + cnz > kNnzTile ||
+                   cur.ncones >= 32000))
+        flush();
+      if (!open) {
+        cur = Task{};
+        cur.rb = (int32_t)a;
+        cur.re = (int32_t)a;
+        cur.nzb = rp[a];
+        cur.nze = rp[a];
+        cur.kind = TASK_ROWS;
+        cur.ncones = 0;
+        cur.cone = (int32_t)k;
+        cur.group = -1;
+        open = true;
+      }
+      cur.re = (int32_t)b;
+      cur.nze = rp[b];
+      cur.ncones++;
+      continue;
+    }
+    flush();
+    int32_t slot = (int32_t)plan.big.size();
+    BigCone bc;
+    bc.cone = (int32_t)k;
+    bc.rb = (int32_t)a;
+    bc.re = (int32_t)b;
+    bc.nparts = 0;
+    plan.big.push_back(bc);
+    int64_t q = a;
+    while (q < b) {
+      int64_t rn = (int64_t)rp[q + 1] - rp[q];
+      if (rn > kNnzTile) {
+        emit_long_row(rp, (int32_t)q, slot, (int32_t)k, plan, multi);
+        plan.big[slot].nparts++;
+        q++;
+        continue;
+      }
+      int64_t start = q, cnt = 0, nz = 0;
+      while (q < b && cnt < kRowCap) {
+        int64_t rq = (int64_t)rp[q + 1] - rp[q];
+        if (rq > kNnzTile) break;
+        if (nz + rq > kNnzTile && cnt > 0) break;
+        nz += rq;
+        cnt++;
+        q++;
+      }
+      Task t{};
+      t.rb = (int32_t)start;
+      t.re = (int32_t)q;
+      t.nzb = rp[start];
+      t.nze = rp[q];
+      t.kind = TASK_CONE_PART;
+      t.ncones = 0;
+      t.cone = (int32_t)k;
+      t.group = slot;
+      multi.push_back(t);
+      plan.big[slot].nparts++;
+    }
+  }
+  flush();
+  plan.tasks = multi;
+  plan.tasks.insert(plan.tasks.end(), rows.begin(), rows.end());
+}
+
+}  // namespace hpr

@@ -1,0 +1,337 @@
+/*
+ * hprsocp_b200.h — C ABI of the B200 (sm_100a) dual Halpern Peaceman–Rachford
+ * (HPR) iteration for convex quadratic second-order cone programs
+ *
+ *     min  1/2 x'Qx + c'x
+ *     s.t. AL <= A1 x <= AU,   A2 x - b2 in K_soc,   l <= x1 <= u,   x2 in K_var.
+ *
+ * The problem is given in the reference solver's canonical ordering
+ * (src/utils/builders.jl:8-22 of PolyU-IOR/HPR-SOCP): linear rows of A first
+ * (equalities, then inequalities), second-order-cone rows last; boxed variables
+ * first, cone variables last, each cone contiguous.  Cone blocks are described
+ * by start-index vectors exactly like the reference's `SOC_con_idx` /
+ * `SOC_var_idx` (src/structs.jl:139-149), in either 0- or 1-based form.
+ *
+ * Everything crossing this boundary is plain C: pointers, sizes and status
+ * codes.  No C++ exception, CUDA type or torch type appears here.  The library
+ * copies every host array it is given; it owns all device memory until
+ * hpr_destroy().  There is no CPU fallback: without a usable CUDA device every
+ * call returns HPR_E_CUDA.
+ *
+ * Each entry point names the reference function whose device-side role it
+ * takes over (file:line within the reference project).
+ */
+#ifndef HPRSOCP_B200_H
+#define HPRSOCP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+#define HPR_OK 0
+#define HPR_E_CUDA 1      /* CUDA runtime error or no usable device          */
+#define HPR_E_BUDGET 2    /* request exceeds the context's HBM budget        */
+#define HPR_E_BAD_INPUT 3 /* malformed CSR, cone index, size, NaN input ...  */
+#define HPR_E_NUMERIC 4   /* NaN/Inf appeared in residuals or iterates       */
+#define HPR_E_TIMEOUT 5   /* a bounded device wait gave up                   */
+#define HPR_E_STATE 6     /* call order violated (e.g. iterate before upload) */
+#define HPR_E_UNSUPPORTED 7
+
+/* ------------------------------------------------------------------------ */
+/* Problem data                                                              */
+/* ------------------------------------------------------------------------ */
+typedef struct hpr_csr {
+  int64_t nrows;
+  int64_t ncols;
+  int64_t nnz;
+  const int32_t* rowptr; /* nrows+1 entries, offset by index_base          */
+  const int32_t* colind; /* nnz entries, offset by index_base, sorted/row  */
+  const double* values;  /* nnz entries                                    */
+} hpr_csr;
+
+/* How the quadratic term is given.
+ *  NONE         : Q = 0 (the reference's "no-Q" path, has_quadratic_terms false)
+ *  CSR          : explicit sparse symmetric Q; scaled with A; a diagonal CSR Q
+ *                 is detected as in check_Q_diagonal (src/utils/scaling.jl:1312)
+ *  DIAG_LOWRANK : operator Q = diag(q_diag) + F'F, never formed.  Like the
+ *                 reference's user AbstractQOperator, an operator Q disables
+ *                 all scaling (src/utils/scaling.jl:800-846).                */
+#define HPR_Q_NONE 0
+#define HPR_Q_CSR 1
+#define HPR_Q_DIAG_LOWRANK 2
+
+typedef struct hpr_problem {
+  int64_t m;            /* rows of A                                       */
+  int64_t n;            /* columns of A / variables                        */
+  int64_t m_lin;        /* number_linear_con: rows 0..m_lin-1 are linear   */
+  int64_t n_box;        /* number_lu_x: when variable cones exist, only    */
+                        /* variables 0..n_box-1 are boxed                  */
+  hpr_csr A;            /* m x n                                           */
+  hpr_csr AT;           /* optional n x m transpose of A, as the reference */
+                        /* keeps it (QP_info_cpu.AT); rowptr == NULL means */
+                        /* "build it on upload"                            */
+  const double* c;      /* n                                               */
+  const double* l;      /* n (entries of cone variables are ignored)       */
+  const double* u;      /* n                                               */
+  const double* AL;     /* m (-inf allowed)                                */
+  const double* AU;     /* m (+inf allowed)                                */
+  const double* soc_rhs;/* m - m_lin: b2, aligned with the cone rows       */
+  const int64_t* soc_con_idx; /* cone row starts + end sentinel           */
+  int64_t n_soc_con_idx;      /* length (#constraint cones + 1), >= 1      */
+  const int64_t* soc_var_idx; /* cone variable starts + end sentinel      */
+  int64_t n_soc_var_idx;      /* length (#variable cones + 1), >= 1        */
+  int32_t index_base;   /* 0 (C) or 1 (Julia) for every index above        */
+  int32_t q_kind;       /* HPR_Q_*                                          */
+  hpr_csr Q;            /* n x n when q_kind == HPR_Q_CSR                   */
+  const double* q_diag; /* n when q_kind == HPR_Q_DIAG_LOWRANK              */
+  hpr_csr F;            /* k x n factor when q_kind == HPR_Q_DIAG_LOWRANK   */
+  double obj_constant;
+} hpr_problem;
+
+/* ------------------------------------------------------------------------ */
+/* Parameters and results (fields mirror HPRSOCP_parameters and             */
+/* HPRSOCP_results, src/structs.jl:208-314)                                  */
+/* ------------------------------------------------------------------------ */
+#define HPR_BC_NORM_L2 0
+#define HPR_BC_NORM_RMS 1
+#define HPR_BC_NORM_LINF 2
+
+/* SOC block-scaling strategies (src/utils/scaling.jl:150-227).             */
+#define HPR_SOC_SCALE_MAX 1
+#define HPR_SOC_SCALE_RMS 2
+#define HPR_SOC_SCALE_GEOM 3
+#define HPR_SOC_SCALE_ADAPTIVE 4
+#define HPR_SOC_SCALE_HYBRID 5
+#define HPR_SOC_SCALE_RUIZ_GEOM 6
+#define HPR_SOC_SCALE_ROLE_SPLIT 7
+#define HPR_SOC_SCALE_POCK_SAFE_ROLE_SPLIT 8
+#define HPR_SOC_SCALE_SIZE_SPLIT_ROLE_SPLIT 9
+#define HPR_SOC_SCALE_PRE_POCK_SIZE_SPLIT 10
+#define HPR_SOC_SCALE_PRE_POCK_HUGE_VAR_TAPER 11
+#define HPR_SOC_SCALE_PRE_POCK_HUGE_VAR_TAPER_POCK_GEOM 12
+#define HPR_SOC_SCALE_PRE_POCK_BAND_SPLIT 13
+#define HPR_SOC_SCALE_PRE_POCK_CONSTRAINT_RMS 14
+#define HPR_SOC_SCALE_PRE_POCK_CONSTRAINT_MAX 15
+#define HPR_SOC_SCALE_PRE_POCK_CONSTRAINT_TAPER 16
+#define HPR_SOC_SCALE_SMALL_CONE_CONSTRAINT_MAX 17
+#define HPR_SOC_SCALE_COUNT_AWARE_SMALL_CONE_BIAS 18
+#define HPR_SOC_SCALE_PHASE_BLEND 19
+#define HPR_SOC_SCALE_PHASE_TAPER 20
+
+/* Arithmetic of the A / A' SpMV stream (hpr_set_precision).               */
+#define HPR_PREC_FP64 0      /* FP64 values, FP64 accumulation (reference)  */
+#define HPR_PREC_FP32 1      /* FP32 values and gathers, FP64 epilogue      */
+#define HPR_PREC_BF16 2      /* BF16 values, FP32 accumulation, FP64 epilogue */
+
+typedef struct hpr_params {
+  double stoptol;        /* 1e-6                                            */
+  double sigma;          /* -1 = automatic ||b||/||c|| (algorithm.jl:1538)  */
+  int64_t max_iter;      /* typemax(Int32) in the reference                 */
+  double time_limit;     /* seconds                                         */
+  int64_t check_iter;    /* 150                                             */
+  int64_t print_frequency; /* -1 = adaptive print_step (algorithm.jl:1906)  */
+  int32_t device_number;
+  int32_t use_Ruiz_scaling;
+  int32_t ruiz_iterations;
+  int32_t use_bc_scaling;
+  int32_t bc_scaling_norm_type;       /* HPR_BC_NORM_*                      */
+  int32_t use_Pock_Chambolle_scaling;
+  int32_t soc_block_scaling_strategy; /* HPR_SOC_SCALE_*                    */
+  int32_t verbose;
+  const double* initial_x; /* NULL or n entries (original coordinates)    */
+  const double* initial_y; /* NULL or m entries                            */
+  /* Extensions (no reference counterpart): injected eigenvalue estimates
+   * (values <= 0 mean "estimate by power iteration") and SpMV precision.  */
+  double lambda_max_A;
+  double lambda_max_Q;
+  int32_t precision;       /* HPR_PREC_*                                     */
+  int32_t refine;          /* mixed precision: outer FP64 refinement passes */
+} hpr_params;
+
+#define HPR_STATUS_OPTIMAL 0
+#define HPR_STATUS_MAX_ITER 1
+#define HPR_STATUS_TIME_LIMIT 2
+
+typedef struct hpr_residuals {
+  double err_Rp_org_bar;
+  double err_Rp_linear_org_bar;
+  double err_Rp_soc_org_bar;
+  double err_Rd_org_bar;
+  double KKTx_and_gap_org_bar;
+  double primal_obj_bar;
+  double rel_gap_bar;
+  double dual_obj_bar;
+} hpr_residuals;
+
+typedef struct hpr_results {
+  int64_t iter, iter_4, iter_6;
+  double time, time_4, time_6, power_time;
+  double primal_obj, residuals, gap;
+  int32_t status;          /* HPR_STATUS_*                                   */
+  int32_t restarts;
+  double sigma_final, lambda_max_A, lambda_max_Q;
+  hpr_residuals last;      /* residuals at the final check                   */
+  double* x; /* caller-owned output buffers (may be NULL): n, m, n, n        */
+  double* y;
+  double* z;
+  double* w;
+} hpr_results;
+
+typedef struct hpr_scale_info {
+  double b_scale, c_scale;
+  double norm_b, norm_c, norm_b_org, norm_c_org;
+  int32_t Q_is_diag;
+} hpr_scale_info;
+
+/* Workspace vectors reachable through hpr_get_vector / hpr_set_vector.
+ * All are in the scaled space the iteration runs in.                       */
+#define HPR_VEC_X 0
+#define HPR_VEC_X_BAR 1
+#define HPR_VEC_X_HAT 2
+#define HPR_VEC_LAST_X 3
+#define HPR_VEC_Z_BAR 4
+#define HPR_VEC_Y 5
+#define HPR_VEC_Y_BAR 6
+#define HPR_VEC_LAST_Y 7
+#define HPR_VEC_S 8
+#define HPR_VEC_W 9
+#define HPR_VEC_W_BAR 10
+#define HPR_VEC_LAST_W 11
+#define HPR_VEC_ATY 12
+#define HPR_VEC_LAST_ATY 13
+#define HPR_VEC_DX 14
+#define HPR_VEC_DY 15
+#define HPR_VEC_ROW_NORM 16
+#define HPR_VEC_COL_NORM 17
+#define HPR_VEC_C 18          /* scaled problem data (read-only views)     */
+#define HPR_VEC_AL 19
+#define HPR_VEC_AU 20
+#define HPR_VEC_L 21
+#define HPR_VEC_U 22
+#define HPR_VEC_SOC_RHS 23
+#define HPR_VEC_A_VALUES 24   /* scaled A values (nnz)                     */
+#define HPR_VEC_AT_VALUES 25  /* scaled A' values (nnz)                    */
+#define HPR_VEC_DW 26
+#define HPR_VEC_COUNT 27
+
+typedef struct hpr_ctx hpr_ctx;
+
+/* ------------------------------------------------------------------------ */
+/* Context                                                                   */
+/* ------------------------------------------------------------------------ */
+/* Bind a context to `device` (CUDA.device!, algorithm.jl:2771-2773) with an
+ * HBM budget in bytes (0 = 90% of free memory).  Replaces the device-side
+ * setup of solve() and validate_gpu_parameters! (gpu_validation.jl:16-37),
+ * without its CPU fallback.                                                 */
+int hpr_create(int device, size_t hbm_budget, hpr_ctx** out);
+int hpr_destroy(hpr_ctx* ctx);
+const char* hpr_last_error(const hpr_ctx* ctx);
+const char* hpr_status_string(int code);
+int hpr_version(void);
+
+/* Copy a canonical problem to the device (transfer_to_gpu,
+ * algorithm.jl:2314-2353).  Builds A' on the device, validates every index,
+ * plans the fused SpMV/cone tiles (replacing the SOC bucket planner,
+ * algorithm.jl:1914-2223) and allocates the workspace (allocate_workspace,
+ * algorithm.jl:1443-1588).                                                  */
+int hpr_upload(hpr_ctx* ctx, const hpr_problem* prob);
+
+/* Ruiz / SOC block aggregation / Pock–Chambolle / b-c scaling on the device
+ * (scaling!, src/utils/scaling.jl:785-1289) followed by check_Q_diagonal
+ * (scaling.jl:1312-1353).  May be called once per upload.                   */
+int hpr_scale(hpr_ctx* ctx, const hpr_params* opts, hpr_scale_info* out);
+
+/* Power iteration for lambda_max(AA') and lambda_max(Q)
+ * (power_iteration_A / _Q, src/utils/eigenvalues.jl:68-196).  Returns the
+ * raw estimate; the caller applies the 1.05 safety factor like
+ * estimate_eigenvalues (algorithm.jl:2434-2467).                            */
+int hpr_power_A(hpr_ctx* ctx, int maxit, double tol, double* lambda_out);
+int hpr_power_Q(hpr_ctx* ctx, int maxit, double tol, double* lambda_out);
+
+/* Step size and eigenvalue bounds used by every following iteration; also
+ * refreshes the diagonal-Q factors (unified_update_Q_factors!,
+ * unified_operations.jl:468-498).                                           */
+int hpr_set_sigma_lambda(hpr_ctx* ctx, double sigma, double lambda_A,
+                         double lambda_Q);
+int hpr_set_inner(hpr_ctx* ctx, int64_t inner);
+int hpr_get_scalars(hpr_ctx* ctx, double* sigma, double* lambda_A,
+                    double* lambda_Q, int64_t* inner);
+
+/* Run k HPR iterations (main_update_gpu!, algorithm.jl:2284-2309, with
+ * alpha = 1/(inner+2) and inner incremented after each iteration as in
+ * perform_iteration_step!, algorithm.jl:2722-2744).  When full_last != 0 the
+ * last iteration also writes x_bar, z_bar, dx, s, y_bar, dy (the "full"
+ * kernels used before a residual check).                                    */
+int hpr_iterate(hpr_ctx* ctx, int64_t k, int full_last);
+
+/* KKT residuals of the current (x_bar, y_bar, z_bar[, w_bar]) in original
+ * coordinates (compute_residuals!, algorithm.jl:113-196); include_bounds adds
+ * the iteration-0 bound/cone violation (compute_bounds_violation!,
+ * algorithm.jl:199-256).                                                    */
+int hpr_compute_residuals(hpr_ctx* ctx, int include_bounds,
+                          hpr_residuals* out);
+
+/* Restart gap measure (compute_M_norm!, algorithm.jl:1302-1359), using dx,
+ * dy (and dw) from the last full iteration.                                 */
+int hpr_mnorm(hpr_ctx* ctx, double* out);
+
+/* Inner products of update_sigma! (algorithm.jl:787-833):
+ *   no Q : a = lambda_A*|y_bar-last_y|^2, b = |x_bar-last_x|^2, c = d = 0
+ *   Q    : the a, b, c, d of the reference (diagonal Q: c = d = 0 and the
+ *          sigma search over diag(Q) is hpr_sigma_golden_diag).            */
+int hpr_sigma_terms(hpr_ctx* ctx, double* a, double* b, double* c, double* d);
+
+/* Golden-section search of unified_golden_Q_diag
+ * (unified_operations.jl:411-449) on the device, for diagonal Q.            */
+int hpr_sigma_golden_diag(hpr_ctx* ctx, double a, double b, double lo,
+                          double hi, double tol, double* sigma_out);
+
+/* do_restart! (algorithm.jl:1130-1166): x, last_x <- x_bar; y, last_y <-
+ * y_bar; with Q also w, last_w <- w_bar and ATy, last_ATy <- A'y_bar.       */
+int hpr_restart(hpr_ctx* ctx);
+
+/* Host <-> device copies of workspace vectors (HPR_VEC_*), in the scaled
+ * space.  `len` must equal the vector's length.                            */
+int hpr_get_vector(hpr_ctx* ctx, int which, double* host, size_t len);
+int hpr_set_vector(hpr_ctx* ctx, int which, const double* host, size_t len);
+
+/* Unscaled solution (collect_results!, algorithm.jl:1222-1256): any of the
+ * pointers may be NULL.                                                     */
+int hpr_get_solution(hpr_ctx* ctx, double* x, double* y, double* z, double* w);
+
+/* Precision of the A / A' stream (HPR_PREC_*); re-packs the scaled values.  */
+int hpr_set_precision(hpr_ctx* ctx, int mode);
+
+/* The whole solve (solve(), algorithm.jl:2765-2905): scaling, power
+ * iteration, the restart / sigma loop and unscaling, with the same check,
+ * print and termination schedule.  `res->x/y/z/w` receive the unscaled
+ * solution when non-NULL.                                                   */
+int hpr_solve(hpr_ctx* ctx, const hpr_params* params, hpr_results* res);
+
+/* Convenience: create, upload, solve, destroy in one call (optimize(),
+ * algorithm.jl:2538-2581, without the JIT warm-up which has no meaning for
+ * compiled kernels).                                                        */
+int hpr_optimize(const hpr_problem* prob, const hpr_params* params,
+                 hpr_results* res);
+
+/* Default parameters (HPRSOCP_parameters(), src/structs.jl:277).           */
+void hpr_default_params(hpr_params* p);
+
+/* Device timing of the last hpr_iterate call's kernels, for benchmarks:
+ * total device milliseconds of the x- and y-half kernels.                  */
+int hpr_last_iterate_ms(hpr_ctx* ctx, double* ms_total, int64_t* launches);
+
+/* Algorithmic bytes moved by one partial iteration of the plain path (the
+ * roofline numerator used by the benchmark).                               */
+int hpr_iteration_bytes(hpr_ctx* ctx, double* bytes_per_iter);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HPRSOCP_B200_H */

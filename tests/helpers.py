@@ -1,0 +1,64 @@
+"""Shared helpers of the test suite: KAT loading and array comparison."""
+import json
+import os
+
+import numpy as np
+import scipy.sparse as sp
+
+from hprsocp_b200 import build_from_SOCP_data
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _inf(v):
+    a = np.asarray(v, dtype=np.float64)
+    a[a >= 1e308] = np.inf
+    a[a <= -1e308] = -np.inf
+    return a
+
+
+def load_kats():
+    with open(os.path.join(GOLDEN, "reference_kats.json")) as f:
+        return json.load(f)
+
+
+def kat_model(case):
+    n = len(case["c"])
+    A = sp.csr_matrix(np.array(case["A"], dtype=float).reshape(-1, n)) if case["A"] else sp.csr_matrix((0, n))
+    Q = None if case["Q"] is None else sp.csr_matrix(np.array(case["Q"], dtype=float))
+    return build_from_SOCP_data(Q, np.array(case["c"], dtype=float), A, np.array(case["rhs"], dtype=float),
+                                case["SOC_con_idx"], case["number_eq"], case["number_ineq"], _inf(case["l"]),
+                                _inf(case["u"]), case["SOC_var_idx"], verbose=False)
+
+
+def rel_err(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    if a.size == 0:
+        return 0.0
+    return float(np.max(np.abs(a - b)) / max(1.0, float(np.max(np.abs(b)))))
+
+
+def stress_model(seed=5, with_long_rows=True):
+    """Small instance that exercises every engine path: linear rows longer
+    than one tile (multi-CTA row slices), small cones packed per tile, cones
+    larger than kSmallConeMax and kRowCap (multi-CTA cone slices), a cone
+    containing a long row, and empty rows."""
+    from hprsocp_b200 import instances
+    rng = np.random.default_rng(seed)
+    var_dims = [3] * 400 + [50] * 40 + [300] * 3 + [2500] * 2
+    n_box = 8000
+    n = n_box + int(np.sum(var_dims))
+    m1 = 6000
+    len1 = np.clip(np.rint(np.exp(np.log(10.0) + 1.1 * rng.standard_normal(m1))), 0, 1500).astype(np.int64)
+    if with_long_rows:
+        len1[[7, 1000, 4321]] = [3000, 5000, 2049]
+    len1[[11, 12]] = 0
+    con_dims = [3] * 300 + [40] * 20 + [200] * 3 + [1500]
+    m2 = int(np.sum(con_dims))
+    len2 = rng.integers(3, 12, size=m2)
+    if with_long_rows:
+        len2[m2 - 10] = 4500  # a long row inside the last (large) cone
+    A1 = instances._random_rows(rng, m1, n, len1)
+    A2 = instances._random_rows(rng, m2, n, len2)
+    return instances._assemble(rng, A1, A2, n_box, var_dims, con_dims)

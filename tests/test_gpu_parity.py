@@ -1,0 +1,140 @@
+"""Iterate-level parity of the CUDA path with the FP64 oracle.
+
+Bar (from the workload definition): FP64 iterates within 1e-10 relative after
+a fixed number of iterations with identical sigma and lambda; scaled data
+within 1e-13; residuals/M-norm within 1e-10; full solves reach 1e-6 KKT with
+the objective within 1e-6 relative of the oracle's.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_err, stress_model
+from hprsocp_b200 import HPRSOCP_parameters, instances
+from oracle_ctx import OracleContext
+
+pytestmark = pytest.mark.gpu
+
+ITER_TOL = 1e-10
+SCALE_TOL = 1e-13
+VECS = ["x", "x_hat", "x_bar", "z_bar", "y", "y_bar", "s", "dx", "dy"]
+
+
+@pytest.fixture(scope="module")
+def models():
+    return {"config0": instances.config0(0), "stress": stress_model(5),
+            "config1_small": instances.config1(11, scale=0.004)}
+
+
+def _pair(model):
+    from hprsocp_b200 import Context
+    return OracleContext(model, threads=0), Context(model)
+
+
+def _setup(o, g, params=None):
+    params = params or HPRSOCP_parameters(verbose=False)
+    so = o.scale(params)
+    sg = g.scale(params)
+    lam = o.power_A() * 1.05
+    sigma = so["norm_b"] / so["norm_c"] if so["norm_c"] > 1e-16 else 1.0
+    for c in (o, g):
+        c.set_sigma_lambda(sigma, lam, 0.0)
+        c.set_inner(0)
+    return so, sg
+
+
+@pytest.mark.parametrize("name", ["config0", "stress", "config1_small"])
+def test_scaling_parity(models, name):
+    o, g = _pair(models[name])
+    so = o.scale(HPRSOCP_parameters(verbose=False))
+    sg = g.scale(HPRSOCP_parameters(verbose=False))
+    for k in ("b_scale", "c_scale", "norm_b", "norm_c", "norm_b_org", "norm_c_org"):
+        assert abs(so[k] - sg[k]) <= SCALE_TOL * max(1.0, abs(so[k])), (k, so[k], sg[k])
+    assert so["Q_is_diag"] == sg["Q_is_diag"]
+    for v in ("row_norm", "col_norm", "c", "soc_rhs", "A_values", "AT_values"):
+        assert rel_err(g.get(v), o.get(v)) <= SCALE_TOL, v
+    for v in ("AL", "AU", "l", "u"):
+        a, b = g.get(v), o.get(v)
+        assert np.array_equal(np.isinf(a), np.isinf(b)), v
+        fin = np.isfinite(b)
+        assert rel_err(a[fin], b[fin]) <= SCALE_TOL, v
+
+
+@pytest.mark.parametrize("name", ["config0", "stress", "config1_small"])
+@pytest.mark.parametrize("K", [1, 150, 1000])
+def test_iterate_parity(models, name, K):
+    o, g = _pair(models[name])
+    _setup(o, g)
+    o.iterate(K, True)
+    g.iterate(K, True)
+    for v in VECS:
+        e = rel_err(g.get(v), o.get(v))
+        assert e <= ITER_TOL, (name, K, v, e)
+    assert g.scalars()[3] == o.scalars()[3] == K
+
+
+def test_single_iteration_is_bit_exact_on_serial_rows(models):
+    """Rows of at most 64 nonzeros in one tile and cones of at most 128 rows
+    are summed in the reference's order: one iteration matches bit for bit."""
+    o, g = _pair(models["config0"])
+    _setup(o, g)
+    o.iterate(1, True)
+    g.iterate(1, True)
+    for v in VECS:
+        assert np.array_equal(g.get(v), o.get(v)), v
+
+
+@pytest.mark.parametrize("name", ["config0", "stress"])
+def test_residual_mnorm_sigma_parity(models, name):
+    o, g = _pair(models[name])
+    _setup(o, g)
+    for c in (o, g):
+        c.iterate(149, True)
+    ro = o.residuals(include_bounds=True)
+    rg = g.residuals(include_bounds=True)
+    for k, v in ro.items():
+        assert abs(rg[k] - v) <= 1e-10 * max(1.0, abs(v)), (k, rg[k], v)
+    mo, mg = o.mnorm(), g.mnorm()
+    assert abs(mo - mg) <= 1e-10 * max(1.0, mo)
+    to, tg = o.sigma_terms(), g.sigma_terms()
+    for a, b in zip(to, tg):
+        assert abs(a - b) <= 1e-10 * max(1.0, abs(a))
+
+
+def test_restart_parity(models):
+    o, g = _pair(models["stress"])
+    _setup(o, g)
+    for c in (o, g):
+        c.iterate(150, True)
+        c.restart()
+        c.iterate(75, True)
+    for v in VECS + ["last_x", "last_y"]:
+        assert rel_err(g.get(v), o.get(v)) <= ITER_TOL, v
+
+
+def test_power_iteration_parity(models):
+    o, g = _pair(models["stress"])
+    p = HPRSOCP_parameters(verbose=False)
+    o.scale(p)
+    g.scale(p)
+    lo, lg = o.power_A(), g.power_A()
+    assert abs(lo - lg) <= 1e-6 * lo
+
+
+def test_solve_parity_config0(models):
+    p = HPRSOCP_parameters(verbose=False, stoptol=1e-6, max_iter=100000)
+    o, g = _pair(models["config0"])
+    ro = o.solve(p)
+    rg = g.solve(p)
+    assert ro.status == rg.status == "OPTIMAL"
+    assert rg.residuals <= 1e-6
+    assert abs(rg.primal_obj - ro.primal_obj) <= 1e-6 * max(1.0, abs(ro.primal_obj))
+    assert abs(rg.iter - ro.iter) <= max(10, ro.iter // 20), (rg.iter, ro.iter)
+
+
+def test_solve_is_deterministic(models):
+    from hprsocp_b200 import Context
+    p = HPRSOCP_parameters(verbose=False, stoptol=1e-6, max_iter=3000)
+    r1 = Context(models["stress"]).solve(p)
+    r2 = Context(models["stress"]).solve(p)
+    assert r1.iter == r2.iter
+    assert np.array_equal(r1.x, r2.x) and np.array_equal(r1.y, r2.y)
