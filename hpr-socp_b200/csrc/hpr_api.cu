@@ -17,7 +17,9 @@ int set_err(Ctx* c, int code, const std::string& msg) {
 }
 
 int dev_alloc(Ctx* c, void** p, size_t bytes) {
-  bytes = (bytes + 255) & ~(size_t)255;
+  // +64: tile copies round their byte ranges out to 16-byte boundaries and
+  // may touch up to 15 bytes past the end of an array
+  bytes = (bytes + 64 + 255) & ~(size_t)255;
   if (c->used + bytes > c->budget)
     return set_err(c, HPR_E_BUDGET,
                    "HBM budget exceeded: need " + std::to_string(c->used + bytes) + " of " + std::to_string(c->budget));
@@ -51,6 +53,7 @@ void free_all(Ctx* c) {
     f(p->d_lng_cnt);
     f(p->d_partials);
     f(p->d_raw);
+    f(p->d_ctr);
     *p = Plan();
   }
   double** vs[] = {&c->c,      &c->l,      &c->u,      &c->AL,       &c->AU,     &c->soc_rhs, &c->soc_rhs_full,
@@ -931,6 +934,12 @@ int hpr_set_vector(hpr_ctx* h, int which, const double* host, size_t len) {
   if (L > 0) {
     if (!host) return HPR_E_BAD_INPUT;
     HPR_CUDA(c, cudaMemcpyAsync(p, host, L * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  if (which == HPR_VEC_SOC_RHS && L > 0) {
+    // the kernels read the row-aligned copy (zero on linear rows)
+    HPR_CUDA(c, cudaMemcpyAsync(c->soc_rhs_full + c->m_lin, c->soc_rhs, L * sizeof(double),
+                                cudaMemcpyDeviceToDevice, c->stream));
     HPR_CUDA(c, cudaStreamSynchronize(c->stream));
   }
   if (c->precision != HPR_PREC_FP64 && (which == HPR_VEC_Y || which == HPR_VEC_A_VALUES || which == HPR_VEC_AT_VALUES))

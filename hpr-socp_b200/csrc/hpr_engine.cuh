@@ -3,25 +3,31 @@
 // One launch computes v = M * xin for every row of a matrix side and hands
 // each result to an epilogue functor, so intermediate vectors (A'y, A x_hat,
 // z_raw, s_raw) never reach HBM.  Work comes from the host planner
-// (hpr_plan.cpp) as cone-aligned tiles:
+// (hpr_plan.cpp) as cone-aligned warp tiles of at most kNnzTile nonzeros and
+// kRowCap rows.
 //
-//   1. the tile's nonzeros are streamed with coalesced, evict-first loads of
-//      column indices and values; gathered vector entries come through L2;
-//      products are staged in shared memory;
-//   2. each row is summed from shared memory in ascending column order by one
-//      thread (rows of at most kSerialMax nonzeros — bit-identical to the
-//      reference's sequential sparse product) or by one warp (longer rows);
-//   3. the epilogue runs per row (linear rows / boxed variables) or per cone
-//      (one thread per cone computes ||tail||_2 serially, then one thread per
-//      row projects), or, for cones larger than one tile, in the CTA that
-//      completes the cone's last slice (atomic arrival counter, no waiting);
-//   4. optional reductions (sums and NaN-propagating maxima) are combined in a
-//      fixed order per CTA and written to one slot per tile, so the final
-//      values are independent of scheduling.
-//
-// The last CTA of a launch may also advance the Halpern counter `inner` (an
-// arrival ticket, again with no waiting), which lets a whole iteration run
-// from device-resident scalars and be captured in a CUDA graph.
+// Every warp works on its own tiles with no CTA-wide synchronisation, so the
+// SM's 32+ resident warps hide each other's memory latency.  Persistent
+// warps take tiles (kGrab at a time) from an atomic counter; per tile a warp
+//   0. loads its rows' row pointers and epilogue inputs into registers (two
+//      rows per lane) so their DRAM latency overlaps the gather phase;
+//   1. streams the tile's column indices and values with coalesced
+//      evict-first loads, gathers xin through L2 and writes the products to a
+//      warp-private shared-memory buffer;
+//   2. sums each row from shared memory in ascending column order by one
+//      lane (rows of at most kSerialMax nonzeros — bit-identical to the
+//      reference's sequential sparse product) or by the whole warp;
+//   3. runs the epilogue per row (linear rows / boxed variables) or per cone
+//      (one lane per cone computes ||tail||_2 serially, then one lane per row
+//      projects).  Cones larger than one warp tile and rows longer than one
+//      tile are split over several tiles; the warp that completes the last
+//      slice (atomic arrival counter, no waiting) finishes them;
+//   4. reduces optional scalar reductions in a fixed order and writes one
+//      slot per tile, so results do not depend on scheduling.
+// The last warp to finish resets the tile counter and may advance the
+// Halpern counter `inner`, so a whole iteration runs from device-resident
+// scalars and can be captured in a CUDA graph.  No warp ever waits on
+// another, so the kernel cannot deadlock.
 #pragma once
 
 #include "hpr_internal.h"
@@ -56,18 +62,34 @@ __device__ __forceinline__ void red_combine(Red& a, const Red& b) {
   }
 }
 
-// Fixed-order block reduction; thread 0 returns the result.
+// Fixed-order warp reduction; lane 0 holds the result.
+template <int NRED, unsigned MAXMASK>
+__device__ __forceinline__ void warp_reduce(Red& r) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    Red o;
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) o.v[k] = __shfl_down_sync(0xffffffffu, r.v[k], off);
+    if ((threadIdx.x & 31) + off < 32) red_combine<NRED, MAXMASK>(r, o);
+  }
+}
+
+__device__ __forceinline__ double warp_sum_bcast(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    double o = __shfl_down_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) + off < 32) v = v + o;
+  }
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// Fixed-order block reduction for the plain reduction kernels (kThreads
+// threads); thread 0 returns the result.
 template <int NRED, unsigned MAXMASK>
 __device__ void block_reduce(Red& r, double (*s_red)[kThreads / 32]) {
   if constexpr (NRED > 0) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      Red o;
-#pragma unroll
-      for (int k = 0; k < NRED; ++k) o.v[k] = __shfl_down_sync(0xffffffffu, r.v[k], off);
-      if (lane + off < 32) red_combine<NRED, MAXMASK>(r, o);
-    }
+    warp_reduce<NRED, MAXMASK>(r);
     __syncthreads();
     if (lane == 0)
 #pragma unroll
@@ -89,46 +111,23 @@ __device__ void block_reduce(Red& r, double (*s_red)[kThreads / 32]) {
   }
 }
 
-// Fixed-order block sum of one value per thread; result broadcast to all.
-__device__ __forceinline__ double block_sum_bcast(double v, double* s_tmp) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    double o = __shfl_down_sync(0xffffffffu, v, off);
-    if (lane + off < 32) v = v + o;
-  }
-  __syncthreads();
-  if (lane == 0) s_tmp[wid] = v;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = s_tmp[0];
-    for (int w = 1; w < kThreads / 32; ++w) t = t + s_tmp[w];
-    s_tmp[kThreads / 32] = t;
-  }
-  __syncthreads();
-  double r = s_tmp[kThreads / 32];
-  __syncthreads();
-  return r;
-}
+// The epilogue inputs of one row, read by `in(k, i)` like a vector.
+template <int NS>
+struct Vals {
+  double v[NS > 0 ? NS : 1];
+  __device__ __forceinline__ double operator()(int k, int64_t) const { return v[k]; }
+};
 
-// Matrix values in the precision of the SpMV stream.
-template <int PREC>
-struct ValLoad;
-template <>
-struct ValLoad<HPR_PREC_FP64> {
-  __device__ __forceinline__ static double ld(const DevCSR& M, int64_t e) { return __ldcs(M.val + e); }
-};
-template <>
-struct ValLoad<HPR_PREC_FP32> {
-  __device__ __forceinline__ static double ld(const DevCSR& M, int64_t e) { return (double)__ldcs(M.val32 + e); }
-};
-template <>
-struct ValLoad<HPR_PREC_BF16> {
-  __device__ __forceinline__ static double ld(const DevCSR& M, int64_t e) {
-    unsigned short b = __ldcs(reinterpret_cast<const unsigned short*>(M.val16) + e);
-    return (double)__uint_as_float(((unsigned int)b) << 16);
+// (the source arrays are selected per slot with compile-time indices so the
+// epilogue stays in the kernel-parameter space)
+template <class Epi>
+__device__ __forceinline__ void load_vals(Vals<Epi::kSlots>& o, const Epi& epi, bool cone, int64_t i) {
+#pragma unroll
+  for (int k = 0; k < Epi::kSlots; ++k) {
+    const double* p = cone ? epi.cone_src[k] : epi.lin_src[k];
+    o.v[k] = p ? __ldcs(p + i) : 0.0;
   }
-};
+}
 
 struct EngineArgs {
   DevCSR M;
@@ -140,230 +139,291 @@ struct EngineArgs {
   int bump_inner;       // advance st->inner after the launch
 };
 
-template <class Epi, int PREC>
-__device__ __forceinline__ double gathered_product(const EngineArgs& a, int64_t e, int32_t col) {
-  if constexpr (PREC == HPR_PREC_FP64) {
-    return ValLoad<PREC>::ld(a.M, e) * __ldg(a.xin + col);
+// Matrix values in the precision of the SpMV stream.
+template <int PREC>
+__device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
+  if constexpr (PREC == HPR_PREC_FP32) {
+    return __ldcs(M.val32 + e);
   } else {
-    float v = (float)ValLoad<PREC>::ld(a.M, e);
-    float xv = __ldg(a.xin32 + col);
-    return (double)(v * xv);
+    unsigned short b = __ldcs(reinterpret_cast<const unsigned short*>(M.val16) + e);
+    return __uint_as_float(((unsigned int)b) << 16);
   }
 }
 
+constexpr int kWarpsPerCta = 16;
+constexpr int kEngineThreads = kWarpsPerCta * 32;
+constexpr int kGrab = 2;  // tiles taken per atomic
+constexpr int kChunk = 4; // elements per lane per gather round
+
+struct WarpSmem {
+  double prod[kNnzTile];  // products, later per-cone norms
+  double acc[kRowCap];    // row sums / raw cone values
+  int32_t aux[kRowCap];   // cone heads
+};
+
+__device__ __forceinline__ bool tile_is_cone(const Task& t, bool cones) {
+  return cones && (t.kind == TASK_CONE_PART || t.cone >= 0);
+}
+
+// Finish a cone that was split over several tiles: ||tail||_2 over the raw
+// values (global), then the per-row projection.  Executed by one warp.
 template <class Epi>
-__device__ void finalize_big_cone(const EngineArgs& a, Epi& epi, int slot, double* s_tmp,
-                                  double (*s_red)[kThreads / 32]) {
+__device__ void finalize_big_cone(const EngineArgs& a, Epi& epi, int slot) {
   const BigCone bc = a.pv.big[slot];
   const double* raw = a.pv.raw;
+  const int lane = threadIdx.x & 31;
   __threadfence();
-  // ||tail||_2 with a fixed-order block reduction
   double part = 0.0;
-  for (int r = bc.rb + 1 + threadIdx.x; r < bc.re; r += kThreads) {
+  for (int r = bc.rb + 1 + lane; r < bc.re; r += 32) {
     double v = __ldcg(raw + r);
     part = part + v * v;
   }
-  double ss = block_sum_bcast(part, s_tmp);
-  double ns = sqrt(ss);
+  double ns = sqrt(warp_sum_bcast(part));
   double t = __ldcg(raw + bc.rb);
   Red red;
   red_init<Epi::kNRed, Epi::kMaxMask>(red);
-  for (int r = bc.rb + threadIdx.x; r < bc.re; r += kThreads)
-    epi.cone_apply(r, __ldcg(raw + r), t, ns, r == bc.rb, red);
-  block_reduce<Epi::kNRed, Epi::kMaxMask>(red, s_red);
+  for (int r = bc.rb + lane; r < bc.re; r += 32) {
+    Vals<Epi::kSlots> v;
+    load_vals<Epi>(v, epi, true, r);
+    epi.cone_apply(r, __ldcg(raw + r), t, ns, r == bc.rb, v, red);
+  }
   if constexpr (Epi::kNRed > 0) {
-    if (threadIdx.x == 0) {
+    warp_reduce<Epi::kNRed, Epi::kMaxMask>(red);
+    if (lane == 0) {
       double* dst = a.red_slots + (int64_t)(a.pv.ntasks + slot) * kMaxRed;
       for (int k = 0; k < Epi::kNRed; ++k) dst[k] = red.v[k];
     }
   }
-  if (threadIdx.x == 0) a.pv.big_cnt[slot] = 0;
+  if (lane == 0) a.pv.big_cnt[slot] = 0;
 }
 
-// Arrival on a big cone: returns true (in every thread) for the CTA that
-// completed it.  Callers must have written their raw values.
-__device__ __forceinline__ bool arrive_big(const EngineArgs& a, int slot, int* s_flag) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
+// Arrival of one slice on a split cone; true (in every lane) for the warp
+// that completed it.  Callers must have written their raw values.
+__device__ __forceinline__ bool arrive_big(const EngineArgs& a, int slot) {
+  __threadfence();  // every lane publishes its raw values
+  __syncwarp();
+  int last = 0;
+  if ((threadIdx.x & 31) == 0) {
     int old = atomicAdd(a.pv.big_cnt + slot, 1);
-    *s_flag = (old == a.pv.big[slot].nparts - 1) ? 1 : 0;
+    last = (old == a.pv.big[slot].nparts - 1) ? 1 : 0;
   }
-  __syncthreads();
-  return *s_flag != 0;
+  return __shfl_sync(0xffffffffu, last, 0) != 0;
 }
 
 template <class Epi, int PREC>
-__global__ void __launch_bounds__(kThreads) engine_kernel(EngineArgs a, Epi epi) {
-  __shared__ double s_prod[kNnzTile];
-  __shared__ double s_acc[kRowCap];
-  __shared__ int32_t s_rp[kRowCap + 1];
-  __shared__ int32_t s_aux[kRowCap];
-  __shared__ double s_red[kMaxRed][kThreads / 32];
-  __shared__ double s_tmp[kThreads / 32 + 1];
-  __shared__ int s_nlong;
-  __shared__ int s_flag;
-
-  const Task t = a.pv.tasks[blockIdx.x];
-  epi.setup(a.st);
-  const int tid = threadIdx.x;
+__device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSmem& ws) {
+  const int lane = threadIdx.x & 31;
+  const Task t = a.pv.tasks[tix];
   const int nrows = t.re - t.rb;
   const int nnz = t.nze - t.nzb;
-  Red red;
-  red_init<Epi::kNRed, Epi::kMaxMask>(red);
+  const bool cone = tile_is_cone(t, Epi::kCones);
 
-  // ---- 1. stage row pointers and products
-  if (t.kind != TASK_LONG_PART)
-    for (int r = tid; r <= nrows; r += kThreads) s_rp[r] = __ldg(a.M.rowptr + t.rb + r) - t.nzb;
-  if (tid == 0) s_nlong = 0;
-  {
-    constexpr int U = kNnzTile / kThreads;
-    int32_t cols[U];
-    double prods[U];
-#pragma unroll
-    for (int k = 0; k < U; ++k) {
-      int e = tid + k * kThreads;
-      cols[k] = (e < nnz) ? __ldcs(a.M.col + t.nzb + e) : 0;
+  // ---- 0. row pointers and epilogue inputs of this lane's two rows
+  int r0b = 0, r0e = 0, r1b = 0, r1e = 0;
+  Vals<Epi::kSlots> v0, v1;
+  if (t.kind != TASK_LONG_PART) {
+    if (lane < nrows) {
+      r0b = __ldg(a.M.rowptr + t.rb + lane) - t.nzb;
+      r0e = __ldg(a.M.rowptr + t.rb + lane + 1) - t.nzb;
+      load_vals<Epi>(v0, epi, cone, t.rb + lane);
     }
-#pragma unroll
-    for (int k = 0; k < U; ++k) {
-      int e = tid + k * kThreads;
-      if (e < nnz) prods[k] = gathered_product<Epi, PREC>(a, (int64_t)t.nzb + e, cols[k]);
-    }
-#pragma unroll
-    for (int k = 0; k < U; ++k) {
-      int e = tid + k * kThreads;
-      if (e < nnz) s_prod[e] = prods[k];
+    if (lane + 32 < nrows) {
+      r1b = __ldg(a.M.rowptr + t.rb + lane + 32) - t.nzb;
+      r1e = __ldg(a.M.rowptr + t.rb + lane + 33) - t.nzb;
+      load_vals<Epi>(v1, epi, cone, t.rb + lane + 32);
     }
   }
-  __syncthreads();
 
+  // ---- 1. products into warp-private shared memory
+  for (int c0 = 0; c0 < nnz; c0 += 32 * kChunk) {
+    int32_t cols[kChunk];
+    double vals[kChunk];
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k) {
+      int e = c0 + lane + 32 * k;
+      if (e < nnz) {
+        cols[k] = __ldcs(a.M.col + t.nzb + e);
+        if constexpr (PREC == HPR_PREC_FP64) vals[k] = __ldcs(a.M.val + t.nzb + e);
+        else vals[k] = (double)ldval32<PREC>(a.M, (int64_t)t.nzb + e);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k) {
+      int e = c0 + lane + 32 * k;
+      if (e < nnz) {
+        if constexpr (PREC == HPR_PREC_FP64) ws.prod[e] = vals[k] * __ldg(a.xin + cols[k]);
+        else ws.prod[e] = (double)((float)vals[k] * __ldg(a.xin32 + cols[k]));
+      }
+    }
+  }
+  __syncwarp();
+
+  Red red;
+  red_init<Epi::kNRed, Epi::kMaxMask>(red);
   if (t.kind == TASK_LONG_PART) {
     // ---- partial sum of one long row
     double part = 0.0;
-    for (int e = tid; e < nnz; e += kThreads) part = part + s_prod[e];
-    double ps = block_sum_bcast(part, s_tmp);
+    for (int e = lane; e < nnz; e += 32) part = part + ws.prod[e];
+    double ps = warp_sum_bcast(part);
     const LongRow lr = a.pv.lng[t.group];
-    if (tid == 0) {
+    int last = 0;
+    if (lane == 0) {
       a.pv.partials[lr.partial_base + t.part] = ps;
       __threadfence();
       int old = atomicAdd(a.pv.lng_cnt + t.group, 1);
-      s_flag = (old == lr.nparts - 1) ? 1 : 0;
+      last = (old == lr.nparts - 1) ? 1 : 0;
     }
-    __syncthreads();
-    if (s_flag) {
+    if (__shfl_sync(0xffffffffu, last, 0)) {
       __threadfence();
-      if (tid == 0) {
-        double tot = 0.0;
+      double tot = 0.0;
+      if (lane == 0) {
         for (int p = 0; p < lr.nparts; ++p) tot = tot + __ldcg(a.pv.partials + lr.partial_base + p);
         a.pv.lng_cnt[t.group] = 0;
-        s_tmp[0] = tot;
       }
-      __syncthreads();
-      const double tot = s_tmp[0];
+      const bool to_cone = Epi::kCones && lr.bigcone >= 0;
       Red lred;
       red_init<Epi::kNRed, Epi::kMaxMask>(lred);
-      bool to_cone = Epi::kCones && lr.bigcone >= 0;
-      if (!to_cone) {
-        if (tid == 0) epi.linear(lr.row, tot, lred);
-      } else {
-        if (tid == 0) a.pv.raw[lr.row] = epi.cone_raw(lr.row, tot, lred);
-      }
-      if constexpr (Epi::kNRed > 0) {
-        if (tid == 0) {
+      if (lane == 0) {
+        Vals<Epi::kSlots> v;
+        load_vals<Epi>(v, epi, to_cone, lr.row);
+        if (!to_cone) epi.linear(lr.row, tot, v, lred);
+        else a.pv.raw[lr.row] = epi.cone_raw(lr.row, tot, v, lred);
+        if constexpr (Epi::kNRed > 0) {
           double* dst = a.red_slots + (int64_t)(a.pv.ntasks + a.pv.nbig + t.group) * kMaxRed;
           for (int k = 0; k < Epi::kNRed; ++k) dst[k] = lred.v[k];
         }
       }
-      if (to_cone) {
-        if (arrive_big(a, lr.bigcone, &s_flag)) finalize_big_cone(a, epi, lr.bigcone, s_tmp, s_red);
-      } else if constexpr (Epi::kNRed > 0) {
-        // a big-cone slot of a non-cone epilogue is written by its parts
-      }
+      if (to_cone && arrive_big(a, lr.bigcone)) finalize_big_cone(a, epi, lr.bigcone);
     }
-  } else {
-    // ---- 2. row sums from shared memory
-    for (int r = tid; r < nrows; r += kThreads) {
-      int b0 = s_rp[r], b1 = s_rp[r + 1];
-      if (b1 - b0 <= kSerialMax) {
-        double s = 0.0;
-        for (int k = b0; k < b1; ++k) s = s + s_prod[k];
-        s_acc[r] = s;
-      } else {
-        int li = atomicAdd(&s_nlong, 1);
-        s_aux[li] = r;
-      }
+    if constexpr (Epi::kNRed > 0) {
+      // this tile's own slot carries nothing
+      if (lane == 0)
+        for (int k = 0; k < Epi::kNRed; ++k) a.red_slots[(int64_t)tix * kMaxRed + k] = 0.0;
     }
-    __syncthreads();
-    {
-      const int lane = tid & 31, wid = tid >> 5;
-      for (int li = wid; li < s_nlong; li += kThreads / 32) {
-        int r = s_aux[li];
-        int b0 = s_rp[r], b1 = s_rp[r + 1];
-        double s = 0.0;
-        for (int k = b0 + lane; k < b1; k += 32) s = s + s_prod[k];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) s = s + __shfl_down_sync(0xffffffffu, s, off);
-        if (lane == 0) s_acc[r] = s;
-      }
-    }
-    __syncthreads();
+    return;
+  }
 
-    // ---- 3. epilogue
-    const bool cones_here = Epi::kCones && (t.kind == TASK_CONE_PART || t.cone >= 0);
-    if (!cones_here) {
-      for (int r = tid; r < nrows; r += kThreads) epi.linear(t.rb + r, s_acc[r], red);
-      if constexpr (Epi::kNRed > 0) {
-        if (t.kind == TASK_CONE_PART && tid == 0) {
-          double* dst = a.red_slots + (int64_t)(a.pv.ntasks + t.group) * kMaxRed;
-          for (int k = 0; k < Epi::kNRed; ++k) dst[k] = 0.0;
-        }
-      }
-    } else if (t.kind == TASK_CONE_PART) {
-      for (int r = tid; r < nrows; r += kThreads) a.pv.raw[t.rb + r] = epi.cone_raw(t.rb + r, s_acc[r], red);
-      if (arrive_big(a, t.group, &s_flag)) finalize_big_cone(a, epi, t.group, s_tmp, s_red);
+  // ---- 2. row sums
+  bool long0 = false, long1 = false;
+  if (lane < nrows) {
+    if (r0e - r0b <= kSerialMax) {
+      double s = 0.0;
+      for (int k = r0b; k < r0e; ++k) s = s + ws.prod[k];
+      ws.acc[lane] = s;
     } else {
-      // whole small cones: raw values in place, one thread per cone for the
-      // norm (ascending order, like the reference), one thread per row for
-      // the projection.
-      for (int r = tid; r < nrows; r += kThreads) s_acc[r] = epi.cone_raw(t.rb + r, s_acc[r], red);
-      __syncthreads();
-      double* s_ns = s_prod;  // products are dead; reuse for per-cone norms
-      for (int k = tid; k < t.ncones; k += kThreads) {
-        int c0 = __ldg(a.pv.cone_start + t.cone + k) - t.rb;
-        int c1 = __ldg(a.pv.cone_start + t.cone + k + 1) - t.rb;
-        double ss = 0.0;
-        for (int j = c0 + 1; j < c1; ++j) ss += s_acc[j] * s_acc[j];
-        s_ns[c0] = sqrt(ss);
-        for (int j = c0; j < c1; ++j) s_aux[j] = c0;
-      }
-      __syncthreads();
-      for (int r = tid; r < nrows; r += kThreads) {
-        int h = s_aux[r];
-        epi.cone_apply(t.rb + r, s_acc[r], s_acc[h], s_ns[h], r == h, red);
-      }
+      long0 = true;
     }
   }
+  if (lane + 32 < nrows) {
+    if (r1e - r1b <= kSerialMax) {
+      double s = 0.0;
+      for (int k = r1b; k < r1e; ++k) s = s + ws.prod[k];
+      ws.acc[lane + 32] = s;
+    } else {
+      long1 = true;
+    }
+  }
+  {
+    unsigned m0 = __ballot_sync(0xffffffffu, long0), m1 = __ballot_sync(0xffffffffu, long1);
+    while (m0 | m1) {
+      int src_lane, rr;
+      if (m0) {
+        src_lane = __ffs(m0) - 1;
+        m0 &= m0 - 1;
+        rr = src_lane;
+      } else {
+        src_lane = __ffs(m1) - 1;
+        m1 &= m1 - 1;
+        rr = src_lane + 32;
+      }
+      int b0 = __shfl_sync(0xffffffffu, rr < 32 ? r0b : r1b, src_lane);
+      int b1 = __shfl_sync(0xffffffffu, rr < 32 ? r0e : r1e, src_lane);
+      double s = 0.0;
+      for (int k = b0 + lane; k < b1; k += 32) s = s + ws.prod[k];
+      s = warp_sum_bcast(s);
+      if (lane == 0) ws.acc[rr] = s;
+    }
+  }
+  __syncwarp();
+
+  // ---- 3. epilogue
+  if (!cone) {
+    if (lane < nrows) epi.linear(t.rb + lane, ws.acc[lane], v0, red);
+    if (lane + 32 < nrows) epi.linear(t.rb + lane + 32, ws.acc[lane + 32], v1, red);
+    if constexpr (Epi::kNRed > 0) {
+      if (t.kind == TASK_CONE_PART && lane == 0) {
+        double* dst = a.red_slots + (int64_t)(a.pv.ntasks + t.group) * kMaxRed;
+        for (int k = 0; k < Epi::kNRed; ++k) dst[k] = 0.0;
+      }
+    }
+  } else if (t.kind == TASK_CONE_PART) {
+    if (lane < nrows) a.pv.raw[t.rb + lane] = epi.cone_raw(t.rb + lane, ws.acc[lane], v0, red);
+    if (lane + 32 < nrows) a.pv.raw[t.rb + lane + 32] = epi.cone_raw(t.rb + lane + 32, ws.acc[lane + 32], v1, red);
+    if (arrive_big(a, t.group)) finalize_big_cone(a, epi, t.group);
+  } else {
+    // whole small cones: raw values in place, one lane per cone for the
+    // norm (ascending order, like the reference), one lane per row for the
+    // projection.
+    if (lane < nrows) ws.acc[lane] = epi.cone_raw(t.rb + lane, ws.acc[lane], v0, red);
+    if (lane + 32 < nrows) ws.acc[lane + 32] = epi.cone_raw(t.rb + lane + 32, ws.acc[lane + 32], v1, red);
+    __syncwarp();
+    double* ns = ws.prod;  // products are dead
+    for (int k = lane; k < t.ncones; k += 32) {
+      int c0 = __ldg(a.pv.cone_start + t.cone + k) - t.rb;
+      int c1 = __ldg(a.pv.cone_start + t.cone + k + 1) - t.rb;
+      double ss = 0.0;
+      for (int j = c0 + 1; j < c1; ++j) ss += ws.acc[j] * ws.acc[j];
+      ns[c0] = sqrt(ss);
+      for (int j = c0; j < c1; ++j) ws.aux[j] = c0;
+    }
+    __syncwarp();
+    if (lane < nrows) {
+      int h = ws.aux[lane];
+      epi.cone_apply(t.rb + lane, ws.acc[lane], ws.acc[h], ns[h], lane == h, v0, red);
+    }
+    if (lane + 32 < nrows) {
+      int r = lane + 32, h = ws.aux[r];
+      epi.cone_apply(t.rb + r, ws.acc[r], ws.acc[h], ns[h], r == h, v1, red);
+    }
+  }
+  __syncwarp();
 
   // ---- 4. per-tile reduction slot
   if constexpr (Epi::kNRed > 0) {
-    block_reduce<Epi::kNRed, Epi::kMaxMask>(red, s_red);
-    if (tid == 0) {
-      double* dst = a.red_slots + (int64_t)blockIdx.x * kMaxRed;
+    warp_reduce<Epi::kNRed, Epi::kMaxMask>(red);
+    if (lane == 0) {
+      double* dst = a.red_slots + (int64_t)tix * kMaxRed;
       for (int k = 0; k < Epi::kNRed; ++k) dst[k] = red.v[k];
     }
   }
-  // ---- 5. Halpern counter
-  if (a.bump_inner) {
-    __syncthreads();
-    if (tid == 0) {
+}
+
+constexpr int kEngineSmem = kWarpsPerCta * (int)sizeof(WarpSmem);
+
+template <class Epi, int PREC>
+__global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineArgs a, Epi epi) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmem* s_ws = reinterpret_cast<WarpSmem*>(smem_raw);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int ntasks = a.pv.ntasks;
+  epi.setup(a.st);
+  WarpSmem& ws = s_ws[wid];
+  for (;;) {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(a.pv.task_ctr, kGrab);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= ntasks) break;
+    for (int q = 0; q < kGrab && base + q < ntasks; ++q) process_warp_tile<Epi, PREC>(a, epi, base + q, ws);
+  }
+  // ---- last warp: reset the tile counter, advance the Halpern counter
+  if (lane == 0) {
+    __threadfence();
+    int tk = atomicAdd(a.pv.done_ctr, 1);
+    if (tk == (int)(gridDim.x * kWarpsPerCta) - 1) {
+      *a.pv.task_ctr = 0;
+      *a.pv.done_ctr = 0;
+      if (a.bump_inner) a.st->inner = a.st->inner + 1;
       __threadfence();
-      int tk = atomicAdd(&a.st->ticket, 1);
-      if (tk == (int)gridDim.x - 1) {
-        a.st->inner = a.st->inner + 1;
-        a.st->ticket = 0;
-        __threadfence();
-      }
     }
   }
 }
@@ -411,7 +471,6 @@ __global__ void __launch_bounds__(kThreads) vec_map_kernel(int64_t n, F f) {
   for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) f(i);
 }
 
-
 template <int NRED, unsigned MASK, class F>
 inline int vec_reduce(Ctx* c, int64_t n, F f, int red_off) {
   if (n <= 0) {
@@ -436,10 +495,15 @@ inline int vec_map(Ctx* c, int64_t n, F f) {
   return HPR_OK;
 }
 
+// Read back `count` reduction results (and the device error flag).
 inline int fetch_red(Ctx* c, int count) {
   HPR_CUDA(c, cudaMemcpyAsync(c->h_red_out, c->d_red_out, count * sizeof(double), cudaMemcpyDeviceToHost,
                               c->stream));
+  HPR_CUDA(c, cudaMemcpyAsync(&c->h_state->error, &c->d_state->error, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                              c->stream));
   HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (c->h_state->error != 0)
+    return set_err(c, c->h_state->error, "device error flag set");
   return HPR_OK;
 }
 

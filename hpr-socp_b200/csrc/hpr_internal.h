@@ -5,6 +5,7 @@
 #include <cuda_bf16.h>
 
 #include <cstdint>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -14,16 +15,17 @@ namespace hpr {
 
 // ---------------------------------------------------------------------------
 // Tiling of the fused SpMV + epilogue engine.
-//   A CTA of kThreads threads processes one Task.  kNnzTile products are
-//   staged in shared memory and each row is summed in column order, so the
-//   result of a row whose nonzeros fit one tile is bit-identical to the
-//   reference's sequential CSC/CSR accumulation.
+//   A persistent CTA of kThreads threads processes one Task at a time with
+//   the next one in flight.  A tile's kNnzTile products are formed in shared
+//   memory and each row is summed in column order, so the result of a row
+//   whose nonzeros fit one tile is bit-identical to the reference's
+//   sequential CSC/CSR accumulation.
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;
-constexpr int kNnzTile = 2048;
-constexpr int kRowCap = 1024;
+constexpr int kNnzTile = 512;
+constexpr int kRowCap = 64;
 constexpr int kSerialMax = 64;      // rows longer than this use a warp reduction
-constexpr int kSmallConeMax = 128;  // larger cones take the multi-CTA path
+constexpr int kSmallConeMax = 64;   // larger cones are split over several tiles
 constexpr int kMaxRed = 8;          // reduction lanes per engine launch
 
 enum TaskKind : int16_t {
@@ -64,6 +66,7 @@ struct Plan {
   int32_t* d_lng_cnt = nullptr;
   double* d_partials = nullptr;  // long-row partial sums
   double* d_raw = nullptr;       // big-cone raw values (nrows)
+  int32_t* d_ctr = nullptr;      // [0] tile counter, [1] finished CTAs
   int32_t nslots() const {
     return (int32_t)tasks.size() + (int32_t)big.size() + (int32_t)lng.size();
   }
@@ -106,6 +109,8 @@ struct PlanView {
   double* partials;
   double* raw;
   const int32_t* cone_start;  // cone start rows (+ sentinel), this side
+  int32_t* task_ctr;          // next tile to take
+  int32_t* done_ctr;          // CTAs that finished (last one resets both)
   int32_t ntasks, nbig, nlng;
 };
 

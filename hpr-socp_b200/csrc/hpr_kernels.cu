@@ -22,16 +22,25 @@ __device__ __forceinline__ void halpern(const DevState* st, double& H1, double& 
   H2 = 1.0 - H1;
 }
 
+// Every epilogue declares kSlots per-row input streams.  The engine stages
+// rows [rb, re) of lin_src[k] (linear tiles) or cone_src[k] (cone tiles)
+// into shared memory with the tile, and the epilogue reads them through
+// `in(k, i)`; inputs that are rarely needed are read from global memory.
+
 // ---------------------------------------------------------------------------
 // x half-step without Q: unified_update_zx_kernel_full!/partial!
 // (kernels.jl:5955-6063) and the SOC variable projections (kernels.jl:
 // 1652-1706); CPU twin unified_update_zx_cpu! (kernels.jl:7672-7812).
+// slots: 0 x, 1 last_x, 2 c, 3 l, 4 u
 // ---------------------------------------------------------------------------
 struct EpiX {
   static constexpr bool kCones = true;
   static constexpr int kNRed = 0;
   static constexpr unsigned kMaxMask = 0;
-  const double *c, *l, *u, *last_x;
+  static constexpr int kSlots = 5;
+  using In = Vals<kSlots>;
+  const double* lin_src[kSlots];
+  const double* cone_src[kSlots];
   double *x, *x_hat, *x_bar, *z_bar, *dx;
   float* x_hat32;
   int full;
@@ -40,9 +49,9 @@ struct EpiX {
     sigma = st->sigma;
     halpern(st, H1, H2);
   }
-  __device__ __forceinline__ void finish(int64_t i, double xi, double xb, double zr) {
+  __device__ __forceinline__ void finish(int64_t i, double xi, double lxi, double xb, double zr) {
     double xh = 2.0 * xb - xi;
-    double xn = fma(H2, xh, H1 * last_x[i]);
+    double xn = fma(H2, xh, H1 * lxi);
     if (full) {
       dx[i] = xb - xi;
       x_bar[i] = xb;
@@ -52,15 +61,15 @@ struct EpiX {
     x_hat[i] = xh;
     if (x_hat32) x_hat32[i] = (float)xh;
   }
-  __device__ void linear(int64_t i, double aty, Red&) {
-    double xi = x[i];
-    double tmp = aty - c[i];
+  __device__ void linear(int64_t i, double aty, const In& in, Red&) {
+    double xi = in(0, i);
+    double tmp = aty - in(2, i);
     double zr = xi + sigma * tmp;
-    double xb = cmin(cmax(zr, l[i]), u[i]);
-    finish(i, xi, xb, zr);
+    double xb = cmin(cmax(zr, in(3, i)), in(4, i));
+    finish(i, xi, in(1, i), xb, zr);
   }
-  __device__ double cone_raw(int64_t i, double aty, Red&) { return x[i] + sigma * (aty - c[i]); }
-  __device__ void cone_apply(int64_t i, double zr, double t, double ns, bool head, Red&) {
+  __device__ double cone_raw(int64_t i, double aty, const In& in, Red&) { return in(0, i) + sigma * (aty - in(2, i)); }
+  __device__ void cone_apply(int64_t i, double zr, double t, double ns, bool head, const In& in, Red&) {
     double xb;
     if (ns <= -t) xb = 0.0;
     else if (ns <= t) xb = zr;
@@ -68,7 +77,7 @@ struct EpiX {
       double pt = (ns + t) / 2.0;
       xb = head ? pt : (pt / ns) * zr;
     }
-    finish(i, x[i], xb, zr);
+    finish(i, in(0, i), in(1, i), xb, zr);
   }
 };
 
@@ -76,15 +85,19 @@ struct EpiX {
 // y half-step: unified_update_y_kernel_full!/partial! (kernels.jl:4354-4456)
 // and the SOC constraint projections (kernels.jl:4458-5368); CPU twins
 // unified_update_y_noQ_cpu! (7817-7952) and update_y_cpu! (7976-8096).
+// slots: linear rows 0 y, 1 last_y, 2 AL, 3 AU; cone rows 0 y, 1 last_y,
+// 2 soc_rhs (row-aligned)
 // ---------------------------------------------------------------------------
 struct EpiY {
   static constexpr bool kCones = true;
   static constexpr int kNRed = 0;
   static constexpr unsigned kMaxMask = 0;
-  const double *AL, *AU, *rhs, *last_y;
+  static constexpr int kSlots = 4;
+  using In = Vals<kSlots>;
+  const double* lin_src[kSlots];
+  const double* cone_src[kSlots];
   double *y, *y_bar, *s, *dy;
   float* y32;
-  int64_t m_lin;
   int full, ybar_always;
   double f1, f2, H1, H2;
   __device__ void setup(const DevState* st) {
@@ -92,9 +105,9 @@ struct EpiY {
     f2 = 1.0 / f1;
     halpern(st, H1, H2);
   }
-  __device__ __forceinline__ void finish(int64_t i, double yi, double yb, double sp) {
+  __device__ __forceinline__ void finish(int64_t i, double yi, double lyi, double yb, double sp) {
     double yh = 2.0 * yb - yi;
-    double yn = fma(H2, yh, H1 * last_y[i]);
+    double yn = fma(H2, yh, H1 * lyi);
     if (full) {
       s[i] = sp;
       dy[i] = yb - yi;
@@ -105,16 +118,16 @@ struct EpiY {
     y[i] = yn;
     if (y32) y32[i] = (float)yn;
   }
-  __device__ void linear(int64_t i, double ax, Red&) {
-    double yi = y[i];
+  __device__ void linear(int64_t i, double ax, const In& in, Red&) {
+    double yi = in(0, i);
     double sr = ax - f1 * yi;
-    double sp = cmin(cmax(sr, AL[i]), AU[i]);
+    double sp = cmin(cmax(sr, in(2, i)), in(3, i));
     double corr = sp - sr;
     double yb = f2 * corr;
-    finish(i, yi, yb, sp);
+    finish(i, yi, in(1, i), yb, sp);
   }
-  __device__ double cone_raw(int64_t i, double ax, Red&) { return ax - rhs[i - m_lin] - f1 * y[i]; }
-  __device__ void cone_apply(int64_t i, double sr, double t, double ns, bool head, Red&) {
+  __device__ double cone_raw(int64_t i, double ax, const In& in, Red&) { return ax - in(2, i) - f1 * in(0, i); }
+  __device__ void cone_apply(int64_t i, double sr, double t, double ns, bool head, const In& in, Red&) {
     double sp;
     if (ns <= -t) sp = 0.0;
     else if (ns <= t) sp = sr;
@@ -123,7 +136,7 @@ struct EpiY {
       sp = head ? pt : (pt / ns) * sr;
     }
     double yb = f2 * (sp - sr);
-    finish(i, y[i], yb, sp);
+    finish(i, in(0, i), in(1, i), yb, sp);
   }
 };
 
@@ -132,12 +145,17 @@ struct EpiY {
 // (kernels.jl:379-494) with the SOC-with-Q projections (634-1263); CPU twin
 // update_zxw1_cpu! (7487-7664).  qdiag != null means the operator
 // diag(qdiag) + F'F and `v` is (F'(F w))_i.
+// slots: 0 x, 1 last_x, 2 c, 3 ATy, 4 w, 5 l, 6 u
 // ---------------------------------------------------------------------------
 struct EpiQX {
   static constexpr bool kCones = true;
   static constexpr int kNRed = 0;
   static constexpr unsigned kMaxMask = 0;
-  const double *c, *l, *u, *last_x, *aty, *w, *fact1, *fact2, *qdiag;
+  static constexpr int kSlots = 7;
+  using In = Vals<kSlots>;
+  const double* lin_src[kSlots];
+  const double* cone_src[kSlots];
+  const double *fact1, *fact2, *qdiag;
   double *x, *x_hat, *x_bar, *z_bar, *dx, *w_bar, *Qw;
   int full, diag;
   double sigma, H1, H2, f1s, f2s;
@@ -147,11 +165,14 @@ struct EpiQX {
     f2s = 1.0 / (1.0 + st->sigma * st->lamQ);
     f1s = 1.0 - f2s;
   }
-  __device__ __forceinline__ double qw(int64_t i, double v) { return qdiag ? qdiag[i] * w[i] + v : v; }
-  __device__ __forceinline__ void finish(int64_t i, double xi, double xb, double zr) {
+  __device__ __forceinline__ double qw(int64_t i, double v, const In& in) {
+    return qdiag ? qdiag[i] * in(4, i) + v : v;
+  }
+  __device__ __forceinline__ void finish(int64_t i, const In& in, double xi, double xb, double zr) {
     double xh = 2.0 * xb - xi;
-    double xn = fma(H2, xh, H1 * last_x[i]);
-    w_bar[i] = diag ? fma(fact1[i], w[i], fact2[i] * xh) : fma(f1s, w[i], f2s * xh);
+    double xn = fma(H2, xh, H1 * in(1, i));
+    double wi = in(4, i);
+    w_bar[i] = diag ? fma(fact1[i], wi, fact2[i] * xh) : fma(f1s, wi, f2s * xh);
     if (full) {
       dx[i] = xb - xi;
       x_bar[i] = xb;
@@ -160,21 +181,21 @@ struct EpiQX {
     x[i] = xn;
     x_hat[i] = xh;
   }
-  __device__ void linear(int64_t i, double v, Red&) {
-    double q = qw(i, v);
+  __device__ void linear(int64_t i, double v, const In& in, Red&) {
+    double q = qw(i, v, in);
     Qw[i] = q;
-    double xi = x[i];
-    double tmp = -q + aty[i] - c[i];
+    double xi = in(0, i);
+    double tmp = -q + in(3, i) - in(2, i);
     double zr = xi + sigma * tmp;
-    double xb = cmin(cmax(zr, l[i]), u[i]);
-    finish(i, xi, xb, zr);
+    double xb = cmin(cmax(zr, in(5, i)), in(6, i));
+    finish(i, in, xi, xb, zr);
   }
-  __device__ double cone_raw(int64_t i, double v, Red&) {
-    double q = qw(i, v);
+  __device__ double cone_raw(int64_t i, double v, const In& in, Red&) {
+    double q = qw(i, v, in);
     Qw[i] = q;
-    return x[i] + sigma * (-q + aty[i] - c[i]);
+    return in(0, i) + sigma * (-q + in(3, i) - in(2, i));
   }
-  __device__ void cone_apply(int64_t i, double zr, double t, double ns, bool head, Red&) {
+  __device__ void cone_apply(int64_t i, double zr, double t, double ns, bool head, const In& in, Red&) {
     double xb;
     if (ns <= -t) xb = 0.0;
     else if (ns <= t) xb = zr;
@@ -182,38 +203,48 @@ struct EpiQX {
       double pt = (ns + t) / 2.0;
       xb = head ? pt : (pt / ns) * zr;
     }
-    finish(i, x[i], xb, zr);
+    finish(i, in, in(0, i), xb, zr);
   }
 };
 
 // tempv = x_hat + sigma (Qw - Q w_bar): compute_tempv_unified_kernel!
 // (kernels.jl:4268-4299); CPU update_y_cpu! (kernels.jl:7988-7989).
+// slots: 0 x_hat, 1 Qw, 2 w_bar
 struct EpiQT {
   static constexpr bool kCones = false;
   static constexpr int kNRed = 0;
   static constexpr unsigned kMaxMask = 0;
-  const double *x_hat, *Qw, *w_bar, *qdiag;
+  static constexpr int kSlots = 3;
+  using In = Vals<kSlots>;
+  const double* lin_src[kSlots];
+  const double* cone_src[kSlots];
+  const double* qdiag;
   double* tempv;
   float* tempv32;
   double sigma;
   __device__ void setup(const DevState* st) { sigma = st->sigma; }
-  __device__ void linear(int64_t i, double v, Red&) {
-    double qwb = qdiag ? qdiag[i] * w_bar[i] + v : v;
-    double tv = x_hat[i] + sigma * (Qw[i] - qwb);
+  __device__ void linear(int64_t i, double v, const In& in, Red&) {
+    double qwb = qdiag ? qdiag[i] * in(2, i) + v : v;
+    double tv = in(0, i) + sigma * (in(1, i) - qwb);
     tempv[i] = tv;
     if (tempv32) tempv32[i] = (float)tv;
   }
-  __device__ double cone_raw(int64_t, double v, Red&) { return v; }
-  __device__ void cone_apply(int64_t, double, double, double, bool, Red&) {}
+  __device__ double cone_raw(int64_t, double v, const In&, Red&) { return v; }
+  __device__ void cone_apply(int64_t, double, double, double, bool, const In&, Red&) {}
 };
 
 // w2 half-step: unified_update_w2_kernel_full!/partial! (kernels.jl:
 // 5384-5497); CPU update_w2_cpu! (kernels.jl:8100-8185).
+// slots: 0 w, 1 w_bar, 2 ATy, 3 last_w, 4 last_ATy
 struct EpiW2 {
   static constexpr bool kCones = false;
   static constexpr int kNRed = 0;
   static constexpr unsigned kMaxMask = 0;
-  const double *last_w, *last_aty, *fact;
+  static constexpr int kSlots = 5;
+  using In = Vals<kSlots>;
+  const double* lin_src[kSlots];
+  const double* cone_src[kSlots];
+  const double* fact;
   double *w, *w_bar, *aty, *aty_bar, *dw, *atdy;
   int full, diag;
   double H1, H2, fs;
@@ -221,12 +252,12 @@ struct EpiW2 {
     halpern(st, H1, H2);
     fs = st->sigma / (1.0 + st->sigma * st->lamQ);
   }
-  __device__ void linear(int64_t i, double ab, Red&) {
-    double wi = w[i], wbi = w_bar[i], ai = aty[i];
+  __device__ void linear(int64_t i, double ab, const In& in, Red&) {
+    double wi = in(0, i), wbi = in(1, i), ai = in(2, i);
     double f = diag ? fact[i] : fs;
     double wbn = wbi + f * (ab - ai);
-    double wn = H1 * last_w[i] + H2 * (2.0 * wbn - wi);
-    double an = H1 * last_aty[i] + H2 * (2.0 * ab - ai);
+    double wn = H1 * in(3, i) + H2 * (2.0 * wbn - wi);
+    double an = H1 * in(4, i) + H2 * (2.0 * ab - ai);
     w[i] = wn;
     aty[i] = an;
     if (full) {
@@ -236,8 +267,8 @@ struct EpiW2 {
       aty_bar[i] = ab;
     }
   }
-  __device__ double cone_raw(int64_t, double v, Red&) { return v; }
-  __device__ void cone_apply(int64_t, double, double, double, bool, Red&) {}
+  __device__ double cone_raw(int64_t, double v, const In&, Red&) { return v; }
+  __device__ void cone_apply(int64_t, double, double, double, bool, const In&, Red&) {}
 };
 
 // out = M v (+ diag(qdiag) vin for the diag + F'F operator).
@@ -245,98 +276,117 @@ struct EpiPlain {
   static constexpr bool kCones = false;
   static constexpr int kNRed = 0;
   static constexpr unsigned kMaxMask = 0;
+  static constexpr int kSlots = 0;
+  using In = Vals<kSlots>;
+  const double* lin_src[1];
+  const double* cone_src[1];
   double* out;
   const double *qdiag, *vin;
   __device__ void setup(const DevState*) {}
-  __device__ void linear(int64_t i, double v, Red&) { out[i] = qdiag ? qdiag[i] * vin[i] + v : v; }
-  __device__ double cone_raw(int64_t, double v, Red&) { return v; }
-  __device__ void cone_apply(int64_t, double, double, double, bool, Red&) {}
+  __device__ void linear(int64_t i, double v, const In&, Red&) { out[i] = qdiag ? qdiag[i] * vin[i] + v : v; }
+  __device__ double cone_raw(int64_t, double v, const In&, Red&) { return v; }
+  __device__ void cone_apply(int64_t, double, double, double, bool, const In&, Red&) {}
 };
 
-// out = M v and <out, other>.
+// out = M v and <out, other>.   slots: 0 other
 struct EpiDot {
   static constexpr bool kCones = false;
   static constexpr int kNRed = 1;
   static constexpr unsigned kMaxMask = 0;
+  static constexpr int kSlots = 1;
+  using In = Vals<kSlots>;
+  const double* lin_src[kSlots];
+  const double* cone_src[kSlots];
   double* out;
-  const double* other;
   __device__ void setup(const DevState*) {}
-  __device__ void linear(int64_t i, double v, Red& r) {
+  __device__ void linear(int64_t i, double v, const In& in, Red& r) {
     out[i] = v;
-    r.v[0] = r.v[0] + v * other[i];
+    r.v[0] = r.v[0] + v * in(0, i);
   }
-  __device__ double cone_raw(int64_t, double v, Red&) { return v; }
-  __device__ void cone_apply(int64_t, double, double, double, bool, Red&) {}
+  __device__ double cone_raw(int64_t, double v, const In&, Red&) { return v; }
+  __device__ void cone_apply(int64_t, double, double, double, bool, const In&, Red&) {}
 };
 
 // Dual residual in original coordinates: compute_Rd_kernel! /
 // compute_Rd_noQ_kernel! (kernels.jl:6467-6512) with the objective dots of
 // compute_residuals! (algorithm.jl:113-160).
 // lanes: 0 max|Rd|, 1 max|A'y_org|, 2 max|Qx_org|, 3 c'x, 4 z'x, 5 x'Qx
+// slots: 0 c, 1 z_bar, 2 x_bar, 3 col_norm, 4 Qx (with Q)
 struct EpiRd {
   static constexpr bool kCones = false;
   static constexpr int kNRed = 6;
   static constexpr unsigned kMaxMask = 0x7;
-  const double *c, *z_bar, *x_bar, *col_norm, *Qx;
+  static constexpr int kSlots = 5;
+  using In = Vals<kSlots>;
+  const double* lin_src[kSlots];
+  const double* cone_src[kSlots];
+  int hasq;
   double cs;
   __device__ void setup(const DevState*) {}
-  __device__ void linear(int64_t i, double v, Red& r) {
-    double cn = col_norm[i];
-    double c_org = c[i] * cn * cs;
+  __device__ void linear(int64_t i, double v, const In& in, Red& r) {
+    double cn = in(3, i);
+    double ci = in(0, i), zi = in(1, i), xi = in(2, i);
+    double c_org = ci * cn * cs;
     double a_org = v * cn * cs;
-    double z_org = z_bar[i] * cn * cs;
+    double z_org = zi * cn * cs;
     double rd;
-    if (Qx) {
-      double q_org = Qx[i] * cn * cs;
+    if (hasq) {
+      double qx = in(4, i);
+      double q_org = qx * cn * cs;
       rd = q_org + c_org - a_org - z_org;
       r.v[2] = nanmax(r.v[2], fabs(q_org));
-      r.v[5] = r.v[5] + x_bar[i] * Qx[i];
+      r.v[5] = r.v[5] + xi * qx;
     } else {
       rd = c_org - a_org - z_org;
     }
     r.v[0] = nanmax(r.v[0], fabs(rd));
     r.v[1] = nanmax(r.v[1], fabs(a_org));
-    r.v[3] = r.v[3] + c[i] * x_bar[i];
-    r.v[4] = r.v[4] + z_bar[i] * x_bar[i];
+    r.v[3] = r.v[3] + ci * xi;
+    r.v[4] = r.v[4] + zi * xi;
   }
-  __device__ double cone_raw(int64_t, double v, Red&) { return v; }
-  __device__ void cone_apply(int64_t, double, double, double, bool, Red&) {}
+  __device__ double cone_raw(int64_t, double v, const In&, Red&) { return v; }
+  __device__ void cone_apply(int64_t, double, double, double, bool, const In&, Red&) {}
 };
 
 // Primal residual in original coordinates: compute_Rp_kernel! and
 // compute_Rp_SOC_kernel! (kernels.jl:6523-6585) with the dual-objective dots
 // y's and y'soc_rhs (algorithm.jl:150-153).
 // lanes: 0 max|Rp_lin|, 1 max|Rp_soc|, 2 max|Ax_org|, 3 y's, 4 y'rhs
+// slots: linear rows 0 AL, 1 AU, 2 row_norm, 3 y_bar, 4 s;
+//        cone rows 0 soc_rhs (row-aligned), 2 row_norm, 3 y_bar, 4 s
 struct EpiRp {
   static constexpr bool kCones = true;
   static constexpr int kNRed = 5;
   static constexpr unsigned kMaxMask = 0x7;
-  const double *AL, *AU, *rhs, *rhs_full, *row_norm, *y_bar, *s;
-  int64_t m_lin;
+  static constexpr int kSlots = 5;
+  using In = Vals<kSlots>;
+  const double* lin_src[kSlots];
+  const double* cone_src[kSlots];
   double bs;
   __device__ void setup(const DevState*) {}
-  __device__ void linear(int64_t i, double v, Red& r) {
-    double rn = row_norm[i];
+  __device__ void linear(int64_t i, double v, const In& in, Red& r) {
+    double rn = in(2, i);
     double ax = v * rn * bs;
-    double lo = AL[i] * rn * bs;
-    double hi = AU[i] * rn * bs;
+    double lo = in(0, i) * rn * bs;
+    double hi = in(1, i) * rn * bs;
     double pr = cmin(cmax(ax, lo), hi);
     double rp = pr - ax;
     r.v[0] = nanmax(r.v[0], fabs(rp));
     r.v[2] = nanmax(r.v[2], fabs(ax));
-    r.v[3] = r.v[3] + y_bar[i] * s[i];
-    r.v[4] = r.v[4] + y_bar[i] * rhs_full[i];
+    r.v[3] = r.v[3] + in(3, i) * in(4, i);
   }
-  __device__ double cone_raw(int64_t i, double v, Red& r) {
-    double rn = row_norm[i];
+  __device__ double cone_raw(int64_t i, double v, const In& in, Red& r) {
+    double rn = in(2, i);
     double ax = v * rn * bs;
-    double rt = rhs[i - m_lin] * rn * bs;
+    double rh = in(0, i);
+    double rt = rh * rn * bs;
+    double yb = in(3, i);
     r.v[2] = nanmax(r.v[2], fabs(ax));
-    r.v[3] = r.v[3] + y_bar[i] * s[i];
-    r.v[4] = r.v[4] + y_bar[i] * rhs_full[i];
+    r.v[3] = r.v[3] + yb * in(4, i);
+    r.v[4] = r.v[4] + yb * rh;
     return ax - rt;
   }
-  __device__ void cone_apply(int64_t i, double sr, double t, double ns, bool head, Red& r) {
+  __device__ void cone_apply(int64_t i, double sr, double t, double ns, bool head, const In&, Red& r) {
     double rp;
     if (ns <= -t) rp = sr;
     else if (ns <= t) rp = 0.0;
@@ -368,6 +418,7 @@ int upload_plan(Ctx* c, Plan& p) {
   HPR_TRY(dev_alloc_n(c, &p.d_lng_cnt, (int64_t)p.lng.size()));
   HPR_TRY(dev_alloc_n(c, &p.d_partials, (int64_t)p.npartials));
   HPR_TRY(dev_alloc_n(c, &p.d_raw, p.nrows));
+  HPR_TRY(dev_alloc_n(c, &p.d_ctr, 2));
   if (nt) HPR_CUDA(c, cudaMemcpy(p.d_tasks, p.tasks.data(), nt * sizeof(Task), cudaMemcpyHostToDevice));
   if (!p.big.empty())
     HPR_CUDA(c, cudaMemcpy(p.d_big, p.big.data(), p.big.size() * sizeof(BigCone), cudaMemcpyHostToDevice));
@@ -375,6 +426,7 @@ int upload_plan(Ctx* c, Plan& p) {
     HPR_CUDA(c, cudaMemcpy(p.d_lng, p.lng.data(), p.lng.size() * sizeof(LongRow), cudaMemcpyHostToDevice));
   HPR_CUDA(c, cudaMemset(p.d_big_cnt, 0, std::max<size_t>(1, p.big.size()) * sizeof(int32_t)));
   HPR_CUDA(c, cudaMemset(p.d_lng_cnt, 0, std::max<size_t>(1, p.lng.size()) * sizeof(int32_t)));
+  HPR_CUDA(c, cudaMemset(p.d_ctr, 0, 2 * sizeof(int32_t)));
   int64_t need = (int64_t)p.nslots() * kMaxRed;
   if (need > c->red_slots) {
     if (c->d_red) {
@@ -398,6 +450,8 @@ PlanView view_of(const Plan& p, const int32_t* cone_start) {
   v.partials = p.d_partials;
   v.raw = p.d_raw;
   v.cone_start = cone_start;
+  v.task_ctr = p.d_ctr;
+  v.done_ctr = p.d_ctr + 1;
   v.ntasks = (int32_t)p.tasks.size();
   v.nbig = (int32_t)p.big.size();
   v.nlng = (int32_t)p.lng.size();
@@ -405,6 +459,32 @@ PlanView view_of(const Plan& p, const int32_t* cone_start) {
 }
 
 namespace {
+
+// Persistent grid size of one engine instantiation (resident CTAs per SM x
+// SMs), computed once.
+template <class Epi, int PREC>
+int engine_grid(int* smem_bytes) {
+  static int grid = 0;
+  constexpr int dyn = kEngineSmem;
+  *smem_bytes = dyn;
+  if (grid == 0) {
+    auto k = engine_kernel<Epi, PREC>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kEngineThreads, dyn);
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    grid = std::max(1, per_sm) * std::max(1, sms);
+  }
+  return grid;
+}
+
+template <class Epi, int PREC>
+void launch_engine_prec(Ctx* c, int nt, const EngineArgs& a, const Epi& epi) {
+  int dyn = 0;
+  int g = std::min(nt, engine_grid<Epi, PREC>(&dyn));
+  engine_kernel<Epi, PREC><<<g, kEngineThreads, dyn, c->stream>>>(a, epi);
+}
 
 template <class Epi>
 int engine_launch(Ctx* c, const DevCSR& M, const Plan& p, const int32_t* cone_start, const double* xin,
@@ -427,11 +507,11 @@ int engine_launch(Ctx* c, const DevCSR& M, const Plan& p, const int32_t* cone_st
   a.red_slots = with_red ? c->d_red : nullptr;
   a.bump_inner = bump ? 1 : 0;
   if (c->precision == HPR_PREC_FP32 && xin32 && M.val32)
-    engine_kernel<Epi, HPR_PREC_FP32><<<nt, kThreads, 0, c->stream>>>(a, epi);
+    launch_engine_prec<Epi, HPR_PREC_FP32>(c, nt, a, epi);
   else if (c->precision == HPR_PREC_BF16 && xin32 && M.val16)
-    engine_kernel<Epi, HPR_PREC_BF16><<<nt, kThreads, 0, c->stream>>>(a, epi);
+    launch_engine_prec<Epi, HPR_PREC_BF16>(c, nt, a, epi);
   else
-    engine_kernel<Epi, HPR_PREC_FP64><<<nt, kThreads, 0, c->stream>>>(a, epi);
+    launch_engine_prec<Epi, HPR_PREC_FP64>(c, nt, a, epi);
   c->launches++;
   HPR_CUDA(c, cudaGetLastError());
   if (with_red) {
@@ -443,18 +523,24 @@ int engine_launch(Ctx* c, const DevCSR& M, const Plan& p, const int32_t* cone_st
   return HPR_OK;
 }
 
+EpiPlain plain(double* out, const double* qdiag = nullptr, const double* vin = nullptr) {
+  EpiPlain e{};
+  e.out = out;
+  e.qdiag = qdiag;
+  e.vin = vin;
+  return e;
+}
+
 // Q v into out (Qmap!, sparse_matrix_operator.jl:27-51); tmp holds F v for
 // the diag + F'F operator.
 int qmap(Ctx* c, const double* v, double* out, double* tmp) {
   if (c->q_kind == HPR_Q_CSR) {
-    EpiPlain e{out, nullptr, nullptr};
-    return engine_launch(c, c->Q, c->planQ, c->d_var_start, v, nullptr, e, false, false, 0);
+    return engine_launch(c, c->Q, c->planQ, c->d_var_start, v, nullptr, plain(out), false, false, 0);
   }
   if (c->q_kind == HPR_Q_DIAG_LOWRANK) {
-    EpiPlain e1{tmp, nullptr, nullptr};
-    HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, v, nullptr, e1, false, false, 0));
-    EpiPlain e2{out, c->qdiag, v};
-    return engine_launch(c, c->FT, c->planQ, c->d_var_start, tmp, nullptr, e2, false, false, 0);
+    HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, v, nullptr, plain(tmp), false, false, 0));
+    return engine_launch(c, c->FT, c->planQ, c->d_var_start, tmp, nullptr, plain(out, c->qdiag, v), false, false,
+                         0);
   }
   HPR_CUDA(c, cudaMemsetAsync(out, 0, c->n * sizeof(double), c->stream));
   return HPR_OK;
@@ -475,13 +561,6 @@ struct AbsMaxF {
   const double* a;
   __device__ void operator()(int64_t i, Red& r) const { r.v[0] = nanmax(r.v[0], fabs(a[i])); }
 };
-
-int dot(Ctx* c, int64_t n, const double* a, const double* b, double* out) {
-  HPR_TRY(vec_reduce<1, 0>(c, n, DotF{a, b}, 0));
-  HPR_TRY(fetch_red(c, 1));
-  *out = c->h_red_out[0];
-  return HPR_OK;
-}
 
 }  // namespace
 
@@ -519,13 +598,30 @@ int update_q_factors(Ctx* c) {
 
 int launch_iteration(Ctx* c, bool full) {
   const bool fp32 = c->precision != HPR_PREC_FP64;
+  EpiY ey{};
+  if (c->m > 0) {
+    const double* ysrc[4] = {c->y, c->last_y, c->AL, c->AU};
+    const double* ycone[4] = {c->y, c->last_y, c->soc_rhs_full, nullptr};
+    for (int k = 0; k < 4; ++k) {
+      ey.lin_src[k] = ysrc[k];
+      ey.cone_src[k] = ycone[k];
+    }
+    ey.y = c->y;
+    ey.y_bar = c->y_bar;
+    ey.s = c->s;
+    ey.dy = c->dy;
+    ey.y32 = fp32 ? c->g32_m : nullptr;
+    ey.full = full ? 1 : 0;
+    ey.ybar_always = c->has_q ? 1 : 0;
+  }
   if (!c->has_q) {
     // main_update_noQ_soc_gpu! (algorithm.jl:2302-2309)
-    EpiX ex;
-    ex.c = c->c;
-    ex.l = c->l;
-    ex.u = c->u;
-    ex.last_x = c->last_x;
+    EpiX ex{};
+    const double* xsrc[5] = {c->x, c->last_x, c->c, c->l, c->u};
+    for (int k = 0; k < 5; ++k) {
+      ex.lin_src[k] = xsrc[k];
+      ex.cone_src[k] = k < 3 ? xsrc[k] : nullptr;
+    }
     ex.x = c->x;
     ex.x_hat = c->x_hat;
     ex.x_bar = c->x_bar;
@@ -533,36 +629,21 @@ int launch_iteration(Ctx* c, bool full) {
     ex.dx = c->dx;
     ex.x_hat32 = fp32 ? c->g32_n : nullptr;
     ex.full = full ? 1 : 0;
-    HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y, fp32 ? c->g32_m : nullptr, ex,
-                          c->m == 0, false, 0));
-    if (c->m > 0) {
-      EpiY ey;
-      ey.AL = c->AL;
-      ey.AU = c->AU;
-      ey.rhs = c->soc_rhs;
-      ey.last_y = c->last_y;
-      ey.y = c->y;
-      ey.y_bar = c->y_bar;
-      ey.s = c->s;
-      ey.dy = c->dy;
-      ey.y32 = fp32 ? c->g32_m : nullptr;
-      ey.m_lin = c->m_lin;
-      ey.full = full ? 1 : 0;
-      ey.ybar_always = 0;
-      HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->x_hat, fp32 ? c->g32_n : nullptr,
-                            ey, true, false, 0));
-    }
+    HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y, fp32 ? c->g32_m : nullptr, ex, c->m == 0,
+                          false, 0));
+    if (c->m > 0)
+      HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->x_hat, fp32 ? c->g32_n : nullptr, ey, true, false,
+                            0));
     return HPR_OK;
   }
   // Q path: zxw1, y, w2 (algorithm.jl:2291-2295)
   const bool lowrank = c->q_kind == HPR_Q_DIAG_LOWRANK;
-  EpiQX eq;
-  eq.c = c->c;
-  eq.l = c->l;
-  eq.u = c->u;
-  eq.last_x = c->last_x;
-  eq.aty = c->ATy;
-  eq.w = c->w;
+  EpiQX eq{};
+  const double* qsrc[7] = {c->x, c->last_x, c->c, c->ATy, c->w, c->l, c->u};
+  for (int k = 0; k < 7; ++k) {
+    eq.lin_src[k] = qsrc[k];
+    eq.cone_src[k] = k < 5 ? qsrc[k] : nullptr;
+  }
   eq.fact1 = c->fact1;
   eq.fact2 = c->fact2;
   eq.qdiag = lowrank ? c->qdiag : nullptr;
@@ -576,46 +657,30 @@ int launch_iteration(Ctx* c, bool full) {
   eq.full = full ? 1 : 0;
   eq.diag = c->Q_is_diag ? 1 : 0;
   if (lowrank) {
-    EpiPlain ef{c->ftmp, nullptr, nullptr};
-    HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, c->w, nullptr, ef, false, false, 0));
+    HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, c->w, nullptr, plain(c->ftmp), false, false, 0));
     HPR_TRY(engine_launch(c, c->FT, c->planQ, c->d_var_start, c->ftmp, nullptr, eq, false, false, 0));
   } else {
     HPR_TRY(engine_launch(c, c->Q, c->planQ, c->d_var_start, c->w, nullptr, eq, false, false, 0));
   }
   if (c->m > 0) {
-    EpiQT et;
-    et.x_hat = c->x_hat;
-    et.Qw = c->Qw;
-    et.w_bar = c->w_bar;
+    EpiQT et{};
+    const double* tsrc[3] = {c->x_hat, c->Qw, c->w_bar};
+    for (int k = 0; k < 3; ++k) et.lin_src[k] = et.cone_src[k] = tsrc[k];
     et.qdiag = lowrank ? c->qdiag : nullptr;
     et.tempv = c->tempv;
     et.tempv32 = fp32 ? c->g32_n : nullptr;
     if (lowrank) {
-      EpiPlain ef{c->ftmp2, nullptr, nullptr};
-      HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, c->w_bar, nullptr, ef, false, false, 0));
+      HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, c->w_bar, nullptr, plain(c->ftmp2), false, false, 0));
       HPR_TRY(engine_launch(c, c->FT, c->planQ, c->d_var_start, c->ftmp2, nullptr, et, false, false, 0));
     } else {
       HPR_TRY(engine_launch(c, c->Q, c->planQ, c->d_var_start, c->w_bar, nullptr, et, false, false, 0));
     }
-    EpiY ey;
-    ey.AL = c->AL;
-    ey.AU = c->AU;
-    ey.rhs = c->soc_rhs;
-    ey.last_y = c->last_y;
-    ey.y = c->y;
-    ey.y_bar = c->y_bar;
-    ey.s = c->s;
-    ey.dy = c->dy;
-    ey.y32 = fp32 ? c->g32_m : nullptr;
-    ey.m_lin = c->m_lin;
-    ey.full = full ? 1 : 0;
-    ey.ybar_always = 1;
-    HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->tempv, fp32 ? c->g32_n : nullptr, ey,
-                          false, false, 0));
+    HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->tempv, fp32 ? c->g32_n : nullptr, ey, false, false,
+                          0));
   }
-  EpiW2 e2;
-  e2.last_w = c->last_w;
-  e2.last_aty = c->last_ATy;
+  EpiW2 e2{};
+  const double* wsrc[5] = {c->w, c->w_bar, c->ATy, c->last_w, c->last_ATy};
+  for (int k = 0; k < 5; ++k) e2.lin_src[k] = e2.cone_src[k] = wsrc[k];
   e2.fact = c->fact;
   e2.w = c->w;
   e2.w_bar = c->w_bar;
@@ -625,8 +690,7 @@ int launch_iteration(Ctx* c, bool full) {
   e2.atdy = c->ATdy;
   e2.full = full ? 1 : 0;
   e2.diag = c->Q_is_diag ? 1 : 0;
-  return engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, e2,
-                       true, false, 0);
+  return engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, e2, true, false, 0);
 }
 
 int run_iterations(Ctx* c, int64_t k, bool full_last) {
@@ -694,24 +758,20 @@ int launch_residuals(Ctx* c, bool include_bounds, hpr_residuals* r) {
   const bool skipq = !c->has_q;
   // offsets in d_red_out: [0..5] Rd lanes, [8..12] Rp lanes, [16] bounds
   if (!skipq) HPR_TRY(qmap(c, c->x_bar, c->Qx, c->ftmp));
-  EpiRd ed;
-  ed.c = c->c;
-  ed.z_bar = c->z_bar;
-  ed.x_bar = c->x_bar;
-  ed.col_norm = c->col_norm;
-  ed.Qx = skipq ? nullptr : c->Qx;
+  EpiRd ed{};
+  const double* dsrc[5] = {c->c, c->z_bar, c->x_bar, c->col_norm, skipq ? nullptr : c->Qx};
+  for (int k = 0; k < 5; ++k) ed.lin_src[k] = ed.cone_src[k] = dsrc[k];
+  ed.hasq = skipq ? 0 : 1;
   ed.cs = cs;
   HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, ed, false, true, 0));
   if (c->m > 0) {
-    EpiRp ep;
-    ep.AL = c->AL;
-    ep.AU = c->AU;
-    ep.rhs = c->soc_rhs;
-    ep.rhs_full = c->soc_rhs_full;
-    ep.row_norm = c->row_norm;
-    ep.y_bar = c->y_bar;
-    ep.s = c->s;
-    ep.m_lin = c->m_lin;
+    EpiRp ep{};
+    const double* psrc[5] = {c->AL, c->AU, c->row_norm, c->y_bar, c->s};
+    const double* pcone[5] = {c->soc_rhs_full, nullptr, c->row_norm, c->y_bar, c->s};
+    for (int k = 0; k < 5; ++k) {
+      ep.lin_src[k] = psrc[k];
+      ep.cone_src[k] = pcone[k];
+    }
     ep.bs = bs;
     HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->x_bar, nullptr, ep, false, true, 8));
   }
@@ -766,7 +826,9 @@ int launch_mnorm(Ctx* c, double* out) {
     HPR_TRY(vec_reduce<2, 0>(c, c->n, Dot2F{c->dQw, c->dx, c->dQw, c->dQw}, 3));  // [3], [4]=dQw'dQw tmp
   }
   if (c->m > 0) {
-    EpiDot e{c->ATdy, c->dx};
+    EpiDot e{};
+    e.lin_src[0] = e.cone_src[0] = c->dx;
+    e.out = c->ATdy;
     HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->dy, nullptr, e, false, true, 2));
   }
   HPR_TRY(fetch_red(c, 8));
@@ -925,8 +987,8 @@ int launch_restart(Ctx* c) {
     HPR_CUDA(c, cudaMemcpyAsync(c->y, c->y_bar, mb, cudaMemcpyDeviceToDevice, c->stream));
     HPR_CUDA(c, cudaMemcpyAsync(c->last_y, c->y_bar, mb, cudaMemcpyDeviceToDevice, c->stream));
     if (c->has_q) {
-      EpiPlain e{c->ATy_bar, nullptr, nullptr};
-      HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, e, false, false, 0));
+      HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, plain(c->ATy_bar), false, false,
+                            0));
       HPR_CUDA(c, cudaMemcpyAsync(c->last_ATy, c->ATy_bar, nb, cudaMemcpyDeviceToDevice, c->stream));
       HPR_CUDA(c, cudaMemcpyAsync(c->ATy, c->ATy_bar, nb, cudaMemcpyDeviceToDevice, c->stream));
     }
@@ -971,10 +1033,10 @@ int power_generic(Ctx* c, int64_t len, bool isA, int maxit, double tol, double* 
     const double* nzp = out + 20;
     if ((rc = vec_map(c, len, [=] __device__(int64_t i) { q[i] = z[i] / sqrt(*nzp); })) != HPR_OK) break;
     if (isA) {
-      EpiPlain e1{tq, nullptr, nullptr};
-      if ((rc = engine_launch(c, c->AT, c->planX, c->d_var_start, q, nullptr, e1, false, false, 0)) != HPR_OK) break;
-      EpiPlain e2{z, nullptr, nullptr};
-      if ((rc = engine_launch(c, c->A, c->planY, c->d_con_start, tq, nullptr, e2, false, false, 0)) != HPR_OK) break;
+      if ((rc = engine_launch(c, c->AT, c->planX, c->d_var_start, q, nullptr, plain(tq), false, false, 0)) != HPR_OK)
+        break;
+      if ((rc = engine_launch(c, c->A, c->planY, c->d_con_start, tq, nullptr, plain(z), false, false, 0)) != HPR_OK)
+        break;
     } else {
       if ((rc = qmap(c, q, z, c->ftmp)) != HPR_OK) break;
     }
@@ -1075,14 +1137,13 @@ int launch_initial_points(Ctx* c, const double* hx0, const double* hy0) {
     }));
     if (m > 0) {
       if (hq) {
-        EpiPlain e{c->ATy_bar, nullptr, nullptr};
-        HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, e, false, false, 0));
+        HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, plain(c->ATy_bar), false, false,
+                              0));
         HPR_CUDA(c, cudaMemcpyAsync(c->ATy, c->ATy_bar, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
         HPR_CUDA(c, cudaMemcpyAsync(c->last_ATy, c->ATy_bar, n * sizeof(double), cudaMemcpyDeviceToDevice,
                                     c->stream));
       } else {
-        EpiPlain e{c->ATy, nullptr, nullptr};
-        HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, e, false, false, 0));
+        HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, plain(c->ATy), false, false, 0));
       }
     }
     if (hq) HPR_TRY(qmap(c, c->x_bar, c->Qx, c->ftmp));
@@ -1095,8 +1156,7 @@ int launch_initial_points(Ctx* c, const double* hx0, const double* hy0) {
       zb[i] = (xb[i] - zr) / sg;
     }));
     if (m > 0) {
-      EpiPlain e{c->Ax, nullptr, nullptr};
-      HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->x_bar, nullptr, e, false, false, 0));
+      HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->x_bar, nullptr, plain(c->Ax), false, false, 0));
       const double *ax = c->Ax, *yy = c->y, *al = c->AL, *au = c->AU;
       double* s = c->s;
       const double f1 = c->lamA * c->sigma;

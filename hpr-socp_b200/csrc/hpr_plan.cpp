@@ -169,6 +169,16 @@ void build_plan(const std::vector<int32_t>& rp, int64_t nrows,
   flush();
   plan.tasks = multi;
   plan.tasks.insert(plan.tasks.end(), rows.begin(), rows.end());
+  // flag tiles holding rows that need the warp-reduction phase
+  for (Task& t : plan.tasks) {
+    if (t.kind == TASK_LONG_PART) continue;
+    t.part = 0;
+    for (int32_t q = t.rb; q < t.re; ++q)
+      if (rp[q + 1] - rp[q] > kSerialMax) {
+        t.part = 1;
+        break;
+      }
+  }
 }
 
 }  // namespace hpr

@@ -77,6 +77,10 @@ def test_single_iteration_is_bit_exact_on_serial_rows(models):
     are summed in the reference's order: one iteration matches bit for bit."""
     o, g = _pair(models["config0"])
     _setup(o, g)
+    # identical scaled data (b_scale/c_scale are reductions whose last bit
+    # depends on summation order)
+    for v in ("c", "AL", "AU", "l", "u", "soc_rhs", "A_values", "AT_values"):
+        g.set(v, o.get(v))
     o.iterate(1, True)
     g.iterate(1, True)
     for v in VECS:
