@@ -23,10 +23,24 @@ int dev_alloc(Ctx* c, void** p, size_t bytes) {
   if (c->used + bytes > c->budget)
     return set_err(c, HPR_E_BUDGET,
                    "HBM budget exceeded: need " + std::to_string(c->used + bytes) + " of " + std::to_string(c->budget));
-  cudaError_t e = cudaMalloc(p, bytes);
-  if (e != cudaSuccess) return set_err(c, HPR_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  // stream-ordered pool allocation: memory released by an earlier context of
+  // this process is reused instead of being mapped again
+  cudaError_t e = cudaMallocAsync(p, bytes, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // usable from any stream from here on
+  if (e != cudaSuccess) return set_err(c, HPR_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
   c->used += bytes;
+  c->allocs[*p] = bytes;
   return HPR_OK;
+}
+
+void dev_free(Ctx* c, void* p) {
+  if (!p) return;
+  auto it = c->allocs.find(p);
+  if (it != c->allocs.end()) {
+    c->used -= it->second;
+    c->allocs.erase(it);
+  }
+  cudaFreeAsync(p, c->stream);
 }
 
 namespace {
@@ -34,9 +48,7 @@ namespace {
 using std::vector;
 
 void free_all(Ctx* c) {
-  auto f = [](void* p) {
-    if (p) cudaFree(p);
-  };
+  auto f = [c](void* p) { dev_free(c, p); };
   for (DevCSR* M : {&c->A, &c->AT, &c->Q, &c->F, &c->FT}) {
     f(M->rowptr);
     f(M->col);
@@ -80,6 +92,8 @@ void free_all(Ctx* c) {
   c->graph_partial = nullptr;
   c->graph_iters = 0;
   c->red_slots = 0;
+  for (auto& kv : c->allocs) cudaFreeAsync(kv.first, c->stream);  // anything not listed above
+  c->allocs.clear();
   c->used = 0;
   c->uploaded = c->scaled = false;
 }
@@ -93,89 +107,6 @@ bool nonan_all(const double* v, int64_t n) {
   for (int64_t i = 0; i < n; ++i)
     if (std::isnan(v[i])) return false;
   return true;
-}
-
-// Validated 0-based host copy of a CSR matrix with sorted rows.
-int load_csr(Ctx* c, const hpr_csr& s, int base, int64_t nr, int64_t nc, const char* name, vector<int32_t>& rp,
-             vector<int32_t>& ci, vector<double>& v) {
-  if (s.nrows != nr || s.ncols != nc)
-    return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": dimensions do not match the problem");
-  if (s.nnz < 0 || s.nnz > (int64_t)std::numeric_limits<int32_t>::max())
-    return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": nnz out of range");
-  if (nr > 0 && !s.rowptr) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": null rowptr");
-  if (s.nnz > 0 && (!s.colind || !s.values)) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": null arrays");
-  rp.resize(nr + 1);
-  ci.resize(s.nnz);
-  v.resize(s.nnz);
-  if (nr == 0) {
-    rp[0] = 0;
-    if (s.nnz != 0) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": nonzeros without rows");
-    return HPR_OK;
-  }
-  for (int64_t i = 0; i <= nr; ++i) rp[i] = s.rowptr[i] - base;
-  if (rp[0] != 0 || rp[nr] != s.nnz) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": rowptr does not span nnz");
-  for (int64_t i = 0; i < nr; ++i)
-    if (rp[i + 1] < rp[i]) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": rowptr decreases");
-  bool sorted = true;
-  for (int64_t i = 0; i < nr; ++i)
-    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
-      int32_t j = s.colind[k] - base;
-      if (j < 0 || j >= nc) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": column index out of range");
-      double x = s.values[k];
-      if (!std::isfinite(x)) return set_err(c, HPR_E_BAD_INPUT, std::string(name) + ": non-finite value");
-      ci[k] = j;
-      v[k] = x;
-      if (k > rp[i] && ci[k] < ci[k - 1]) sorted = false;
-    }
-  if (!sorted) {
-    // order each row by column, as Julia's SparseMatrixCSC always is
-    vector<std::pair<int32_t, double>> tmp;
-    for (int64_t i = 0; i < nr; ++i) {
-      tmp.clear();
-      for (int64_t k = rp[i]; k < rp[i + 1]; ++k) tmp.push_back({ci[k], v[k]});
-      std::stable_sort(tmp.begin(), tmp.end(),
-                       [](const std::pair<int32_t, double>& a, const std::pair<int32_t, double>& b) {
-                         return a.first < b.first;
-                       });
-      for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
-        ci[k] = tmp[k - rp[i]].first;
-        v[k] = tmp[k - rp[i]].second;
-      }
-    }
-  }
-  return HPR_OK;
-}
-
-void transpose(int64_t nr, int64_t nc, const vector<int32_t>& rp, const vector<int32_t>& ci, const vector<double>& v,
-               vector<int32_t>& trp, vector<int32_t>& tci, vector<double>& tv) {
-  trp.assign(nc + 1, 0);
-  for (size_t k = 0; k < ci.size(); ++k) trp[ci[k] + 1]++;
-  for (int64_t j = 0; j < nc; ++j) trp[j + 1] += trp[j];
-  tci.resize(ci.size());
-  tv.resize(v.size());
-  vector<int32_t> pos(trp.begin(), trp.end() - 1);
-  for (int64_t i = 0; i < nr; ++i)
-    for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
-      int32_t p = pos[ci[k]]++;
-      tci[p] = (int32_t)i;
-      tv[p] = v[k];
-    }
-}
-
-int put_csr(Ctx* c, DevCSR& M, int64_t nr, int64_t nc, const vector<int32_t>& rp, const vector<int32_t>& ci,
-            const vector<double>& v) {
-  M.nrows = nr;
-  M.ncols = nc;
-  M.nnz = (int64_t)ci.size();
-  HPR_TRY(dev_alloc_n(c, &M.rowptr, nr + 1));
-  HPR_TRY(dev_alloc_n(c, &M.col, M.nnz));
-  HPR_TRY(dev_alloc_n(c, &M.val, M.nnz));
-  HPR_CUDA(c, cudaMemcpy(M.rowptr, rp.data(), (nr + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
-  if (M.nnz) {
-    HPR_CUDA(c, cudaMemcpy(M.col, ci.data(), M.nnz * sizeof(int32_t), cudaMemcpyHostToDevice));
-    HPR_CUDA(c, cudaMemcpy(M.val, v.data(), M.nnz * sizeof(double), cudaMemcpyHostToDevice));
-  }
-  return HPR_OK;
 }
 
 int put_vec(Ctx* c, double** d, const double* h, int64_t n) {
@@ -383,13 +314,41 @@ int capture_partial_graph(Ctx* c, int G) {
   return HPR_OK;
 }
 
+// Termination message and SOLUTION SUMMARY (handle_termination,
+// algorithm.jl:1740-1790).
+void print_summary(int status, const hpr_residuals& rs, int64_t iter, double solve_s, double setup_s) {
+  static const char* names[] = {"OPTIMAL", "MAX_ITER", "TIME_LIMIT"};
+  const char* st = (status >= 0 && status <= 2) ? names[status] : "UNKNOWN";
+  if (status == HPR_STATUS_OPTIMAL) std::printf("The instance is solved, the accuracy is %.6e\n", rs.KKTx_and_gap_org_bar);
+  else if (status == HPR_STATUS_MAX_ITER)
+    std::printf("The maximum number of iterations is reached, the accuracy is %.6e\n", rs.KKTx_and_gap_org_bar);
+  else if (status == HPR_STATUS_TIME_LIMIT)
+    std::printf("The time limit is reached, the accuracy is %.6e\n", rs.KKTx_and_gap_org_bar);
+  const std::string bar(80, '=');
+  std::printf("\n%s\nSOLUTION SUMMARY\n%s\n", bar.c_str(), bar.c_str());
+  std::printf("Status: %s\nIterations: %lld\nTime: %.2f seconds\n", st, (long long)iter, solve_s);
+  std::printf("Primal Objective: %.12e\nDual Objective: %.12e\n", rs.primal_obj_bar, rs.dual_obj_bar);
+  std::printf("Primal Residual: %.6e\nPrimal Residual (Linear): %.6e\nPrimal Residual (SOC): %.6e\n",
+              rs.err_Rp_org_bar, rs.err_Rp_linear_org_bar, rs.err_Rp_soc_org_bar);
+  std::printf("Dual Residual: %.6e\nRelative Gap: %.6e\n%s\n", rs.err_Rd_org_bar, rs.rel_gap_bar, bar.c_str());
+  std::printf("Total time: %.2fs  (setup = %.2fs, solve = %.2fs)\n%s\n", setup_s + solve_s, setup_s, solve_s,
+              bar.c_str());
+  std::fflush(stdout);
+}
+
 }  // namespace
 
 int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
   if (P->sigma != -1 && !(P->sigma > 0)) return set_err(c, HPR_E_BAD_INPUT, "invalid sigma");
   if (P->print_frequency != -1 && P->print_frequency <= 0) return set_err(c, HPR_E_BAD_INPUT, "invalid print_frequency");
   if (P->check_iter <= 0) return set_err(c, HPR_E_BAD_INPUT, "invalid check_iter");
-  if (!c->scaled) HPR_TRY(run_scaling(c, P, nullptr));
+  double scaling_s = 0.0;
+  if (!c->scaled) {
+    const double ts = now_s();
+    HPR_TRY(run_scaling(c, P, nullptr));
+    scaling_s = now_s() - ts;
+    if (P->verbose) std::printf("GPU SCALING time: %.2f seconds\n", scaling_s);
+  }
   // sigma (allocate_workspace, algorithm.jl:1531-1551)
   double sigma = 1.0;
   if (P->sigma == -1) {
@@ -418,6 +377,7 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
     }
   }
   const double power_time = now_s() - t0;
+  if (P->verbose) std::printf("ESTIMATING MAXIMUM EIGENVALUES time = %.2f seconds\n", power_time);
   c->sigma = sigma;
   c->lamA = lamA;
   c->lamQ = lamQ;
@@ -516,6 +476,7 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
     out->last = rs;
     HPR_TRY(launch_unscale(c, out->x, out->y, out->z, out->w));
   }
+  if (P->verbose) print_summary(status, rs, iter, tt, c->upload_s + scaling_s);
   return HPR_OK;
 }
 
@@ -618,6 +579,18 @@ int hpr_create(int device, size_t budget, hpr_ctx** out) {
     delete h;
     return HPR_E_CUDA;
   }
+  {
+    // keep freed device memory in this process's default pool so a later
+    // context reuses it; its idle part counts as free for the budget
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = ~0ull, reserved = 0, inuse = 0;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+          cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &inuse) == cudaSuccess && reserved > inuse)
+        fr += (size_t)(reserved - inuse);
+    }
+  }
   c->budget = budget ? budget : (size_t)(0.9 * (double)fr);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
@@ -650,6 +623,7 @@ const char* hpr_last_error(const hpr_ctx* h) { return h ? h->c.err.c_str() : "nu
 int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   if (!h || !p) return HPR_E_BAD_INPUT;
   Ctx* c = C(h);
+  const double t_up = now_s();
   cudaSetDevice(c->device);
   free_all(c);
   const int base = p->index_base;
@@ -679,40 +653,35 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   } else {
     c->h_var_idx.assign(1, n);
   }
-  // A and A'
-  vector<int32_t> rp, ci, trp, tci;
-  vector<double> v, tv;
-  HPR_TRY(load_csr(c, p->A, base, m, n, "A", rp, ci, v));
-  if (p->AT.rowptr) HPR_TRY(load_csr(c, p->AT, base, n, m, "AT", trp, tci, tv));
-  else transpose(m, n, rp, ci, v, trp, tci, tv);
-  if ((int64_t)tci.size() != (int64_t)ci.size()) return set_err(c, HPR_E_BAD_INPUT, "AT nnz differs from A");
-  HPR_TRY(put_csr(c, c->A, m, n, rp, ci, v));
-  HPR_TRY(put_csr(c, c->AT, n, m, trp, tci, tv));
+  // A and A' (validated, index-base converted and transposed on the device)
+  vector<int32_t> rp, trp;
+  HPR_TRY(upload_csr(c, p->A, base, m, n, "A", c->A, rp));
+  if (p->AT.rowptr) {
+    HPR_TRY(upload_csr(c, p->AT, base, n, m, "AT", c->AT, trp));
+    if (c->AT.nnz != c->A.nnz) return set_err(c, HPR_E_BAD_INPUT, "AT nnz differs from A");
+  } else {
+    HPR_TRY(transpose_csr(c, c->A, c->AT, trp));
+  }
   c->h_A_rowptr = rp;
   c->h_AT_rowptr = trp;
   // Q
   c->q_kind = p->q_kind;
   c->has_q = false;
-  vector<int32_t> qrp, qci;
-  vector<double> qv;
+  vector<int32_t> qrp;
   if (p->q_kind == HPR_Q_CSR) {
-    HPR_TRY(load_csr(c, p->Q, base, n, n, "Q", qrp, qci, qv));
-    if (qci.empty()) {
+    HPR_TRY(upload_csr(c, p->Q, base, n, n, "Q", c->Q, qrp));
+    if (c->Q.nnz == 0) {
       c->q_kind = HPR_Q_NONE;
     } else {
       c->has_q = true;
-      HPR_TRY(put_csr(c, c->Q, n, n, qrp, qci, qv));
     }
   } else if (p->q_kind == HPR_Q_DIAG_LOWRANK) {
     if (!p->q_diag) return set_err(c, HPR_E_BAD_INPUT, "q_diag is null");
     if (!finite_all(p->q_diag, n)) return set_err(c, HPR_E_BAD_INPUT, "q_diag has non-finite entries");
     int64_t k = p->F.nrows;
-    vector<int32_t> frp, fci, ftrp, ftci;
-    vector<double> fv, ftv;
-    HPR_TRY(load_csr(c, p->F, base, k, n, "F", frp, fci, fv));
-    transpose(k, n, frp, fci, fv, ftrp, ftci, ftv);
-    HPR_TRY(put_csr(c, c->F, k, n, frp, fci, fv));
-    HPR_TRY(put_csr(c, c->FT, n, k, ftrp, ftci, ftv));
+    vector<int32_t> frp, ftrp;
+    HPR_TRY(upload_csr(c, p->F, base, k, n, "F", c->F, frp));
+    HPR_TRY(transpose_csr(c, c->F, c->FT, ftrp));
     HPR_TRY(put_vec(c, &c->qdiag, p->q_diag, n));
     c->has_q = true;
     qrp = ftrp;
@@ -772,7 +741,8 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   HPR_TRY(zero_vec(c, &c->d_red_out, 64));
   int64_t need = (int64_t)kRedGrid * kMaxRed;
   if (need > c->red_slots) {
-    if (c->d_red) cudaFree(c->d_red);
+    dev_free(c, c->d_red);
+    c->d_red = nullptr;
     HPR_TRY(dev_alloc_n(c, &c->d_red, need));
     c->red_slots = need;
   }
@@ -791,6 +761,7 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   HPR_CUDA(c, cudaStreamSynchronize(c->stream));
   c->uploaded = true;
   c->scaled = false;
+  c->upload_s = now_s() - t_up;
   return HPR_OK;
 }
 
@@ -993,6 +964,7 @@ int hpr_optimize(const hpr_problem* prob, const hpr_params* params, hpr_results*
   int rc = hpr_create(params->device_number, 0, &h);
   if (rc != HPR_OK) return rc;
   rc = hpr_upload(h, prob);
+  if (rc == HPR_OK && params->verbose) std::printf("COPY TO GPU time: %.2f seconds\n", C(h)->upload_s);
   if (rc == HPR_OK) rc = hpr_solve(h, params, res);
   if (rc != HPR_OK && params->verbose) std::fprintf(stderr, "hpr_optimize: %s\n", hpr_last_error(h));
   hpr_destroy(h);

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <type_traits>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/hprsocp_b200.h"
@@ -118,6 +119,7 @@ struct Ctx {
   std::string err;
   int device = 0;
   size_t budget = 0, used = 0;
+  std::unordered_map<void*, size_t> allocs;  // live device allocations and their sizes
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool uploaded = false, scaled = false;
@@ -176,6 +178,7 @@ struct Ctx {
   int graph_iters = 0;
   // timing
   double last_ms = 0;
+  double upload_s = 0;  // wall time of the last hpr_upload (COPY TO GPU time)
   int64_t last_launches = 0;
   int64_t launches = 0;
 };
@@ -196,6 +199,7 @@ int set_err(Ctx* c, int code, const std::string& msg);
   } while (0)
 
 int dev_alloc(Ctx* c, void** p, size_t bytes);
+void dev_free(Ctx* c, void* p);  // stream-ordered; tolerates null
 template <class T>
 int dev_alloc_n(Ctx* c, T** p, int64_t n) {
   return dev_alloc(c, (void**)p, (size_t)(n > 0 ? n : 1) * sizeof(T));
@@ -220,6 +224,12 @@ int launch_unscale(Ctx* c, double* x, double* y, double* z, double* w);
 int launch_initial_points(Ctx* c, const double* x0, const double* y0);
 int repack_values(Ctx* c);
 double iteration_bytes(const Ctx* c);
+// device-side CSR ingest (hpr_upload.cu): validates s, converts it to 0-based
+// indices in HBM and returns the 0-based row pointers on the host
+int upload_csr(Ctx* c, const hpr_csr& s, int base, int64_t nr, int64_t nc, const char* name, DevCSR& M,
+               std::vector<int32_t>& rp);
+// deterministic transpose on the device; trp receives T's row pointers
+int transpose_csr(Ctx* c, const DevCSR& M, DevCSR& T, std::vector<int32_t>& trp);
 // scaling (hpr_scale.cu)
 int run_scaling(Ctx* c, const hpr_params* p, hpr_scale_info* out);
 

@@ -429,10 +429,8 @@ int upload_plan(Ctx* c, Plan& p) {
   HPR_CUDA(c, cudaMemset(p.d_ctr, 0, 2 * sizeof(int32_t)));
   int64_t need = (int64_t)p.nslots() * kMaxRed;
   if (need > c->red_slots) {
-    if (c->d_red) {
-      cudaFree(c->d_red);
-      c->used -= (size_t)c->red_slots * sizeof(double);
-    }
+    dev_free(c, c->d_red);
+    c->d_red = nullptr;
     c->red_slots = 0;
     HPR_TRY(dev_alloc_n(c, &c->d_red, need));
     c->red_slots = need;

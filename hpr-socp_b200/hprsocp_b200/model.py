@@ -115,15 +115,19 @@ class SOCPModel:
         s.values = _abi.dptr(v)
         return s
 
-    def to_c(self) -> _abi.hpr_problem:
-        """A struct pointing at this model's arrays (kept alive by the model)."""
+    def to_c(self, with_transpose: bool = False) -> _abi.hpr_problem:
+        """A struct pointing at this model's arrays (kept alive by the model).
+
+        A' is formed on the device unless ``with_transpose`` passes the
+        model's own copy (the reference's QP_info_cpu.AT)."""
         keep: list = []
         p = _abi.hpr_problem()
         p.m, p.n = self.A.shape
         p.m_lin = int(self.number_linear_con)
         p.n_box = int(self.number_lu_x)
         p.A = self._csr_struct(self.A, keep)
-        p.AT = self._csr_struct(self.AT, keep)
+        if with_transpose:
+            p.AT = self._csr_struct(self.AT, keep)
         for name in ("c", "l", "u", "AL", "AU", "soc_rhs"):
             arr = np.ascontiguousarray(getattr(self, name), dtype=np.float64)
             keep.append(arr)
@@ -151,9 +155,11 @@ class SOCPModel:
         self._keep = keep
         return p
 
-    def nbytes(self) -> int:
+    def nbytes(self, with_transpose: bool = False) -> int:
+        """Bytes ``to_c(with_transpose)`` hands to the library."""
         b = self.A.data.nbytes + self.A.indices.nbytes + self.A.indptr.nbytes
-        b += self.AT.data.nbytes + self.AT.indices.nbytes + self.AT.indptr.nbytes
+        if with_transpose:
+            b += self.AT.data.nbytes + self.AT.indices.nbytes + self.AT.indptr.nbytes
         for name in ("c", "AL", "AU", "l", "u", "soc_rhs"):
             b += getattr(self, name).nbytes
         return b

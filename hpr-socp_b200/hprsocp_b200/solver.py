@@ -128,7 +128,10 @@ def results_from_c(r: _abi.hpr_results, x, y, z, w) -> HPRSOCP_results:
 class Context:
     """One device context holding one uploaded problem (hpr_create/upload)."""
 
-    def __init__(self, model: SOCPModel, device: int = 0, budget: int = 0):
+    def __init__(self, model: SOCPModel, device: int = 0, budget: int = 0, problem=None,
+                 with_transpose: bool = False):
+        """``problem`` uploads a caller-built hpr_problem (whose arrays the
+        caller keeps alive) instead of ``model.to_c(with_transpose)``."""
         self.lib = _abi.load_library()
         self.model = model
         h = C.c_void_p()
@@ -136,7 +139,7 @@ class Context:
         if rc != _abi.HPR_OK:
             raise _abi.HPRError(rc, self.lib.hpr_status_string(rc).decode())
         self.h = h
-        self._prob = model.to_c()
+        self._prob = problem if problem is not None else model.to_c(with_transpose)
         self._check(self.lib.hpr_upload(self.h, C.byref(self._prob)))
 
     # -- plumbing ---------------------------------------------------------------
