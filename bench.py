@@ -101,23 +101,28 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_init(n_gpus):
+def dist_init(n_gpus, backend=None):
+    """One process per GPU (torchrun): NCCL on GPUs, gloo for CPU tests."""
     if n_gpus <= 1 or "RANK" not in os.environ:
         return 0, 1, None
     import datetime
     import torch
     import torch.distributed as dist
     rank, world = int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"])
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+    if backend == "nccl":
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return rank, world, dist
 
 
 def dist_max(dist, v):
+    """Max of a per-rank value over all ranks (device timing is max-over-ranks)."""
     if dist is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -125,6 +130,12 @@ def dist_max(dist, v):
 def barrier(dist):
     if dist is not None:
         dist.barrier()
+
+
+def aggregate(world, steps, ms_max):
+    """Whole-job rate of N replicas: all ranks' iterations over the slowest
+    rank's device time."""
+    return world * steps / (ms_max / 1e3)
 
 
 def cpu_iteration_rate(model, iters=3, threads=0):
@@ -220,7 +231,7 @@ def main():
     ms = dist_max(dist, ms)
     bytes_iter = ctx.iteration_bytes()
     ctx.close()
-    value = world * args.steps / (ms / 1e3)
+    value = aggregate(world, args.steps, ms)
     per_iter_ms = ms / args.steps
     peak, peak_kind = measured_peak()
     achieved = bytes_iter / (per_iter_ms / 1e3) / 1e9

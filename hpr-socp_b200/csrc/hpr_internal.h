@@ -16,11 +16,12 @@ namespace hpr {
 
 // ---------------------------------------------------------------------------
 // Tiling of the fused SpMV + epilogue engine.
-//   A persistent CTA of kThreads threads processes one Task at a time with
-//   the next one in flight.  A tile's kNnzTile products are formed in shared
-//   memory and each row is summed in column order, so the result of a row
-//   whose nonzeros fit one tile is bit-identical to the reference's
-//   sequential CSC/CSR accumulation.
+//   One warp processes one Task (tile) at a time: at most kNnzTile nonzeros
+//   of at most kRowCap consecutive rows.  The tile's products are formed in
+//   the warp's shared-memory buffer and each row of at most kSerialMax
+//   nonzeros is summed in column order by one lane, so its result is
+//   bit-identical to the reference's sequential CSC/CSR accumulation.
+//   kThreads is the block size of the plain reduction and map kernels.
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;
 constexpr int kNnzTile = 512;
@@ -67,7 +68,7 @@ struct Plan {
   int32_t* d_lng_cnt = nullptr;
   double* d_partials = nullptr;  // long-row partial sums
   double* d_raw = nullptr;       // big-cone raw values (nrows)
-  int32_t* d_ctr = nullptr;      // [0] tile counter, [1] finished CTAs
+  int32_t* d_ctr = nullptr;      // [0] tile counter, [1] finished warps
   int32_t nslots() const {
     return (int32_t)tasks.size() + (int32_t)big.size() + (int32_t)lng.size();
   }
