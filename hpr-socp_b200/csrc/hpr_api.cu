@@ -845,6 +845,14 @@ int hpr_compute_residuals(hpr_ctx* h, int include_bounds, hpr_residuals* out) {
   return launch_residuals(c, include_bounds != 0, out);
 }
 
+int hpr_compute_residuals_noalloc(hpr_ctx* h, int include_bounds, hpr_residuals* out) {
+  if (!h || !out) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  if (cudaSetDevice(c->device) != cudaSuccess) return set_err(c, HPR_E_CUDA, "cudaSetDevice failed");
+  return launch_residuals_noalloc(c, include_bounds != 0, out);
+}
+
 int hpr_mnorm(hpr_ctx* h, double* out) {
   if (!h || !out) return HPR_E_BAD_INPUT;
   Ctx* c = C(h);

@@ -212,6 +212,7 @@ PlanView view_of(const Plan& p, const int32_t* cone_start);
 int launch_iteration(Ctx* c, bool full);
 int run_iterations(Ctx* c, int64_t k, bool full_last);
 int launch_residuals(Ctx* c, bool include_bounds, hpr_residuals* out);
+int launch_residuals_noalloc(Ctx* c, bool include_bounds, hpr_residuals* out);
 int launch_mnorm(Ctx* c, double* out);
 int launch_sigma_terms(Ctx* c, double* a, double* b, double* cc, double* d);
 int launch_golden_diag(Ctx* c, double a, double b, double lo, double hi,

@@ -7,6 +7,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "hpr_engine.cuh"
 
@@ -1210,6 +1212,147 @@ double iteration_bytes(const Ctx* c) {
   b += m * 24.0 + (double)c->m_lin * 16.0 + (m - (double)c->m_lin) * 8.0;  // y r/w, last_y; AL, AU; rhs
   if (c->precision != HPR_PREC_FP64) b += (n + m) * 4.0;  // FP32 copies written
   return b;
+}
+
+
+// ---------------------------------------------------------------------------
+// Allocation-free residual evaluation (hpr_compute_residuals_noalloc).
+//
+// Same kernels and reduction order as launch_residuals, but the per-tile
+// reduction slots, the per-block partials of the bound check and the result
+// lanes live in a file-scope device array instead of the context's
+// reduction buffers, and the read-back goes to the caller's stack instead of
+// the context's pinned buffer.  Nothing here starts at zero: every slot is
+// written by the tile (or finishing warp) that owns it before
+// final_reduce_kernel reads it, so the array needs no initialisation and
+// carries nothing from one call to the next.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t kNoAllocScratchBytes = (int64_t)2 << 20;  // 2 MiB
+constexpr int64_t kNoAllocDoubles = kNoAllocScratchBytes / (int64_t)sizeof(double);
+constexpr int64_t kNoAllocOut = 24;  // result lanes at the end of the array
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+std::mutex g_noalloc_mu[kNoAllocMaxDevices];  // one call at a time per device
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch on the current device, looked up once.
+int noalloc_scratch(Ctx* c, double** out) {
+  double*& p = g_noalloc_ptr[c->device];
+  if (!p) {
+    void* a = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return set_err(c, HPR_E_CUDA, std::string("cudaGetSymbolAddress(residual scratch): ") + cudaGetErrorString(e));
+    p = static_cast<double*>(a);
+  }
+  *out = p;
+  return HPR_OK;
+}
+
+// engine_launch with caller-given reduction slots and result lanes.
+template <class Epi>
+int engine_launch_into(Ctx* c, const DevCSR& M, const Plan& p, const int32_t* cone_start, const double* xin,
+                       const Epi& epi, double* slots, double* out) {
+  const int nt = (int)p.tasks.size();
+  if (nt == 0) {
+    HPR_CUDA(c, cudaMemsetAsync(out, 0, Epi::kNRed * sizeof(double), c->stream));
+    return HPR_OK;
+  }
+  EngineArgs a;
+  a.M = M;
+  a.xin = xin;
+  a.xin32 = nullptr;
+  a.pv = view_of(p, cone_start);
+  a.st = c->d_state;
+  a.red_slots = slots;
+  a.bump_inner = 0;
+  launch_engine_prec<Epi, HPR_PREC_FP64>(c, nt, a, epi);
+  c->launches++;
+  HPR_CUDA(c, cudaGetLastError());
+  final_reduce_kernel<Epi::kNRed, Epi::kMaxMask><<<1, kThreads, 0, c->stream>>>(slots, p.nslots(), out);
+  c->launches++;
+  HPR_CUDA(c, cudaGetLastError());
+  return HPR_OK;
+}
+
+}  // namespace
+
+int launch_residuals_noalloc(Ctx* c, bool include_bounds, hpr_residuals* r) {
+  if (c->device < 0 || c->device >= kNoAllocMaxDevices)
+    return set_err(c, HPR_E_UNSUPPORTED, "hpr_compute_residuals_noalloc: device ordinal above 63");
+  if (c->precision != HPR_PREC_FP64)
+    return set_err(c, HPR_E_UNSUPPORTED, "hpr_compute_residuals_noalloc: needs the FP64 stream (hpr_set_precision 0)");
+  const int64_t slots = std::max<int64_t>(std::max<int64_t>(c->planX.nslots(), c->planY.nslots()), kRedGrid);
+  const int64_t need = slots * kMaxRed + kNoAllocOut;
+  if (need > kNoAllocDoubles)
+    return set_err(c, HPR_E_UNSUPPORTED,
+                   "hpr_compute_residuals_noalloc: the tile plan needs " + std::to_string(need * 8) +
+                       " bytes of reduction scratch; the static scratch holds " +
+                       std::to_string(kNoAllocScratchBytes) + " (use hpr_compute_residuals)");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu[c->device]);
+  double* scratch = nullptr;
+  HPR_TRY(noalloc_scratch(c, &scratch));
+  double* out = scratch + (kNoAllocDoubles - kNoAllocOut);
+  const double bs = c->b_scale, cs = c->c_scale;
+  const bool skipq = !c->has_q;
+  // lanes of `out`: [0..5] Rd, [8..12] Rp, [16] bounds (as launch_residuals)
+  if (!skipq) HPR_TRY(qmap(c, c->x_bar, c->Qx, c->ftmp));
+  EpiRd ed{};
+  const double* dsrc[5] = {c->c, c->z_bar, c->x_bar, c->col_norm, skipq ? nullptr : c->Qx};
+  for (int k = 0; k < 5; ++k) ed.lin_src[k] = ed.cone_src[k] = dsrc[k];
+  ed.hasq = skipq ? 0 : 1;
+  ed.cs = cs;
+  HPR_TRY(engine_launch_into(c, c->AT, c->planX, c->d_var_start, c->y_bar, ed, scratch, out));
+  if (c->m > 0) {
+    EpiRp ep{};
+    const double* psrc[5] = {c->AL, c->AU, c->row_norm, c->y_bar, c->s};
+    const double* pcone[5] = {c->soc_rhs_full, nullptr, c->row_norm, c->y_bar, c->s};
+    for (int k = 0; k < 5; ++k) {
+      ep.lin_src[k] = psrc[k];
+      ep.cone_src[k] = pcone[k];
+    }
+    ep.bs = bs;
+    HPR_TRY(engine_launch_into(c, c->A, c->planY, c->d_con_start, c->x_bar, ep, scratch, out + 8));
+  }
+  if (include_bounds) {
+    bounds_box_kernel<<<592, kThreads, 0, c->stream>>>(c->n, c->l, c->u, c->x_bar, c->col_norm, bs, c->dx);
+    int64_t nv = (int64_t)c->h_var_idx.size() - 1;
+    if (nv > 0)
+      bounds_cone_kernel<<<(int)std::min<int64_t>((nv + 127) / 128, 1184), 128, 0, c->stream>>>(
+          nv, c->d_var_start, c->x_bar, c->col_norm, bs, c->dx);
+    HPR_CUDA(c, cudaGetLastError());
+    const int64_t len = c->n;
+    vec_reduce_kernel<1, 1, AbsMaxF><<<kRedGrid, kThreads, 0, c->stream>>>(len, AbsMaxF{c->dx}, scratch);
+    final_reduce_kernel<1, 1><<<1, kThreads, 0, c->stream>>>(scratch, kRedGrid, out + 16);
+    HPR_CUDA(c, cudaGetLastError());
+  }
+  double h[17];
+  HPR_CUDA(c, cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  auto jmax = [](double a, double b) { return (a != a) ? a : ((b != b) ? b : (a > b ? a : b)); };
+  double qx_dot = skipq ? 0.0 : h[5];
+  r->primal_obj_bar = bs * cs * (h[3] + 0.5 * qx_dot) + c->obj_constant;
+  r->dual_obj_bar = bs * cs * (-0.5 * qx_dot + h[4]) + c->obj_constant;
+  if (c->m > 0) r->dual_obj_bar += bs * cs * (h[11] + h[12]);
+  r->rel_gap_bar = std::fabs(r->primal_obj_bar - r->dual_obj_bar) /
+                   (1.0 + std::max(std::fabs(r->primal_obj_bar), std::fabs(r->dual_obj_bar)));
+  double qx_inf = skipq ? 0.0 : h[2];
+  r->err_Rd_org_bar = h[0] / (1.0 + jmax(jmax(c->norm_c_org, h[1]), qx_inf));
+  if (c->m > 0) {
+    double denom = 1.0 + jmax(c->norm_b_org, h[10]);
+    r->err_Rp_linear_org_bar = c->m_lin > 0 ? h[8] / denom : 0.0;
+    r->err_Rp_soc_org_bar = c->m_lin < c->m ? h[9] / denom : 0.0;
+    r->err_Rp_org_bar = jmax(h[8], h[9]) / denom;
+  } else {
+    r->err_Rp_org_bar = r->err_Rp_linear_org_bar = r->err_Rp_soc_org_bar = 0.0;
+  }
+  if (include_bounds) r->err_Rp_org_bar = jmax(r->err_Rp_org_bar, h[16]);
+  r->KKTx_and_gap_org_bar = jmax(jmax(r->err_Rp_org_bar, r->err_Rd_org_bar), r->rel_gap_bar);
+  return HPR_OK;
 }
 
 }  // namespace hpr

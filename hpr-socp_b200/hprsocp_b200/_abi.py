@@ -126,6 +126,7 @@ PROTOTYPES = {
     "hpr_get_scalars": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _lp]),
     "hpr_iterate": (C.c_int, [C.c_void_p, C.c_int64, C.c_int]),
     "hpr_compute_residuals": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(hpr_residuals)]),
+    "hpr_compute_residuals_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(hpr_residuals)]),
     "hpr_mnorm": (C.c_int, [C.c_void_p, _dp]),
     "hpr_sigma_terms": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     "hpr_sigma_golden_diag": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,

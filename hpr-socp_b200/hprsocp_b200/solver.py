@@ -213,6 +213,11 @@ class Context:
         self._check(self.lib.hpr_compute_residuals(self.h, int(include_bounds), C.byref(r)))
         return r.as_dict()
 
+    def residuals_noalloc(self, include_bounds: bool = False) -> dict:
+        r = _abi.hpr_residuals()
+        self._check(self.lib.hpr_compute_residuals_noalloc(self.h, int(include_bounds), C.byref(r)))
+        return r.as_dict()
+
     def mnorm(self) -> float:
         v = C.c_double()
         self._check(self.lib.hpr_mnorm(self.h, C.byref(v)))

@@ -277,6 +277,37 @@ int hpr_iterate(hpr_ctx* ctx, int64_t k, int full_last);
 int hpr_compute_residuals(hpr_ctx* ctx, int include_bounds,
                           hpr_residuals* out);
 
+/* The same residuals as hpr_compute_residuals, for callers that must not
+ * allocate after set-up.  No counterpart in the reference.
+ *
+ * Who needs it: a host that runs its own check loop on a device whose memory
+ * is already committed (for example, contexts packed up to their HBM
+ * budgets), or a latency-bound loop that must never enter the CUDA allocator
+ * (cudaMalloc may block; cudaFree and cudaFreeHost synchronise the whole
+ * device and so stall every other stream).  This call allocates nothing: no
+ * device, pinned or pageable allocation, no library routine that allocates.
+ * Its reduction slots and result lanes live in a statically reserved 2 MiB
+ * device array (reserved once per process and device when the library's
+ * CUDA module loads), and its results go through the caller's stack.
+ *
+ * Limits and rules:
+ *  - the problem's tile plan must fit the 2 MiB: at most 32,765 reduction
+ *    slots per matrix side (one per 512-nonzero tile, split cone and long
+ *    row: about 16M nonzeros); larger problems get HPR_E_UNSUPPORTED with
+ *    the sizes in hpr_last_error;
+ *  - FP64 stream only (HPR_E_UNSUPPORTED after hpr_set_precision != 0);
+ *  - nothing in the scratch has to start at zero: every slot is written
+ *    before it is read, and no state survives between calls;
+ *  - all contexts of the process share the scratch of a device, so calls
+ *    that overlapped in time would overwrite each other's partial sums; the
+ *    library therefore serialises the calls per device with a host lock
+ *    held until the results are back (a second caller waits);
+ *  - the first call on a device looks up the scratch's device address
+ *    (cudaGetSymbolAddress, which may load the module); make that first call
+ *    before any stream capture.                                             */
+int hpr_compute_residuals_noalloc(hpr_ctx* ctx, int include_bounds,
+                                  hpr_residuals* out);
+
 /* Restart gap measure (compute_M_norm!, algorithm.jl:1302-1359), using dx,
  * dy (and dw) from the last full iteration.                                 */
 int hpr_mnorm(hpr_ctx* ctx, double* out);
