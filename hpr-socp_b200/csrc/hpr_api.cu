@@ -336,6 +336,21 @@ void print_summary(int status, const hpr_residuals& rs, int64_t iter, double sol
   std::fflush(stdout);
 }
 
+// Precision of the A / A' SpMV stream (hpr_set_precision).  The reduced
+// streams read FP32 / BF16 copies of the scaled values, re-packed here.
+int apply_precision(Ctx* c, int mode) {
+  if (mode != HPR_PREC_FP64 && mode != HPR_PREC_FP32 && mode != HPR_PREC_BF16)
+    return set_err(c, HPR_E_BAD_INPUT, "unknown precision mode");
+  c->precision = mode;
+  if (c->graph_partial) {
+    cudaGraphExecDestroy(c->graph_partial);
+    c->graph_partial = nullptr;
+    c->graph_iters = 0;
+  }
+  if (mode != HPR_PREC_FP64) HPR_TRY(repack_values(c));
+  return HPR_OK;
+}
+
 }  // namespace
 
 int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
@@ -349,6 +364,7 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
     scaling_s = now_s() - ts;
     if (P->verbose) std::printf("GPU SCALING time: %.2f seconds\n", scaling_s);
   }
+  HPR_TRY(apply_precision(c, P->precision));
   // sigma (allocate_workspace, algorithm.jl:1531-1551)
   double sigma = 1.0;
   if (P->sigma == -1) {
@@ -397,6 +413,15 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
   const int64_t ci = P->check_iter;
   int status = -1;
   int64_t iter = 0;
+  // Reduced-precision stream: residuals, restart and sigma logic stay FP64;
+  // the SpMV stream itself switches to FP64 for the finish once the KKT
+  // measure is within `switch_factor` of the tolerance or has stopped
+  // improving (no 20% gain over kStallChecks checks).  refine < 0 keeps the
+  // reduced stream to the end.
+  const double switch_factor = P->refine > 0 ? (double)P->refine : 10.0;
+  constexpr int kStallChecks = 10;
+  double red_best = kInf;
+  int red_stall = 0;
   if (P->verbose) std::printf(" iter     errRp     errRd         p_obj           d_obj          gap        sigma       time\n");
   while (true) {
     // ---- the event iteration `iter` (residual check or print)
@@ -408,6 +433,21 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
     if (rs.KKTx_and_gap_org_bar < P->stoptol) status = HPR_STATUS_OPTIMAL;
     else if (iter == P->max_iter) status = HPR_STATUS_MAX_ITER;
     else if (now_s() - t0 > P->time_limit) status = HPR_STATUS_TIME_LIMIT;
+    if (c->precision != HPR_PREC_FP64 && P->refine >= 0 && status < 0 && iter > 0 && iter % ci == 0) {
+      const double kkt = rs.KKTx_and_gap_org_bar;
+      if (kkt < 0.8 * red_best) {
+        red_best = kkt;
+        red_stall = 0;
+      } else {
+        ++red_stall;
+      }
+      if (kkt < switch_factor * P->stoptol || red_stall >= kStallChecks) {
+        if (P->verbose)
+          std::printf("switching the SpMV stream to FP64 at iteration %lld (KKT %.2e)\n", (long long)iter, kkt);
+        HPR_TRY(apply_precision(c, HPR_PREC_FP64));
+        if (c->A.nnz + c->n + c->m < (int64_t)4000000) HPR_TRY(capture_partial_graph(c, 8));
+      }
+    }
     check_restart(R, iter, ci, c->sigma, rs.KKTx_and_gap_org_bar);
     HPR_TRY(update_sigma(c, R, rs));
     if (R.flag > 0) {
@@ -776,7 +816,10 @@ int hpr_scale(hpr_ctx* h, const hpr_params* opts, hpr_scale_info* out) {
     opts = &d;
   }
   cudaSetDevice(c->device);
-  return run_scaling(c, opts, out);
+  HPR_TRY(run_scaling(c, opts, out));
+  // reduced-precision copies follow the scaled values
+  if (c->precision != HPR_PREC_FP64) HPR_TRY(repack_values(c));
+  return HPR_OK;
 }
 
 int hpr_power_A(hpr_ctx* h, int maxit, double tol, double* lam) {
@@ -939,14 +982,7 @@ int hpr_set_precision(hpr_ctx* h, int mode) {
   HPR_TRY(need_upload(c));
   if (mode != HPR_PREC_FP64 && mode != HPR_PREC_FP32 && mode != HPR_PREC_BF16)
     return set_err(c, HPR_E_BAD_INPUT, "unknown precision mode");
-  c->precision = mode;
-  if (c->graph_partial) {
-    cudaGraphExecDestroy(c->graph_partial);
-    c->graph_partial = nullptr;
-    c->graph_iters = 0;
-  }
-  if (mode != HPR_PREC_FP64) HPR_TRY(repack_values(c));
-  return HPR_OK;
+  return apply_precision(c, mode);
 }
 
 int hpr_solve(hpr_ctx* h, const hpr_params* params, hpr_results* res) {

@@ -46,6 +46,7 @@ class HPRSOCP_parameters:
     lambda_max_A: float = -1.0
     lambda_max_Q: float = -1.0
     precision: str = "fp64"
+    refine: int = 0  # reduced precision: FP64 finish below refine x stoptol (0: 10x); < 0: never
     _keep: list = field(default_factory=list, repr=False)
 
     def to_c(self) -> _abi.hpr_params:
@@ -85,7 +86,7 @@ class HPRSOCP_parameters:
         p.lambda_max_A = self.lambda_max_A
         p.lambda_max_Q = self.lambda_max_Q
         p.precision = _abi.HPR_PREC[self.precision]
-        p.refine = 0
+        p.refine = int(self.refine)
         self._keep = keep
         return p
 
@@ -271,8 +272,6 @@ class Context:
         x, y, z, w = np.zeros(n), np.zeros(m), np.zeros(n), np.zeros(n)
         r = _abi.hpr_results()
         r.x, r.y, r.z, r.w = _abi.dptr(x), _abi.dptr(y), _abi.dptr(z), _abi.dptr(w)
-        if params.precision != "fp64":
-            self.set_precision(params.precision)
         self._check(self.lib.hpr_solve(self.h, C.byref(p), C.byref(r)))
         return results_from_c(r, x, y, z, w)
 

@@ -151,7 +151,12 @@ typedef struct hpr_params {
   double lambda_max_A;
   double lambda_max_Q;
   int32_t precision;       /* HPR_PREC_*                                     */
-  int32_t refine;          /* mixed precision: outer FP64 refinement passes */
+  int32_t refine;          /* reduced-precision solves: the SpMV stream
+                            * switches to FP64 for the finish once the KKT
+                            * measure is below refine x stoptol (refine = 0:
+                            * 10 x stoptol) or stops improving; refine < 0
+                            * keeps the reduced stream to the end.  Residuals,
+                            * restart and sigma logic are FP64 throughout.  */
 } hpr_params;
 
 #define HPR_STATUS_OPTIMAL 0
