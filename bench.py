@@ -189,6 +189,65 @@ def run_reference(args, model, budget_s=150.0):
     print(json.dumps(line))
 
 
+def run_serving(args):
+    """Serving stream: small SOCPs (n lognormal, median 400) with per-request
+    tolerances 1e-4 / 1e-6 through the continuous-batching server, against
+    the same requests solved one at a time with hpr_optimize."""
+    import ctypes as C
+    import numpy as np
+    from hprsocp_b200 import HPRSOCP_parameters, _abi, instances
+    from hprsocp_b200.serving import Server
+    stream = instances.serving_stream(11, args.requests, rate=args.rate)
+    params = [HPRSOCP_parameters(verbose=False, stoptol=tol, max_iter=200000) for _, tol, _ in stream]
+    lib = _abi.load_library()
+    # one at a time: the first `baseline` requests, each a full hpr_optimize
+    nb = min(args.baseline, len(stream))
+    t0 = time.perf_counter()
+    for (model, _, _), p in zip(stream[:nb], params[:nb]):
+        prob, pc = model.to_c(), p.to_c()
+        x, y, z = np.zeros(model.n), np.zeros(model.m), np.zeros(model.n)
+        r = _abi.hpr_results()
+        r.x, r.y, r.z = _abi.dptr(x), _abi.dptr(y), _abi.dptr(z)
+        if lib.hpr_optimize(C.byref(prob), C.byref(pc), C.byref(r)) != 0:
+            raise RuntimeError("hpr_optimize failed")
+    seq_rate = nb / (time.perf_counter() - t0)
+    # the server: requests submitted at their arrival times (all at t = 0 at
+    # saturation), results polled in submission order
+    with Server(slots=args.slots) as srv:
+        for model, p in zip([m for m, _, _ in stream[:2]], params[:2]):   # warm the slots
+            srv.poll(srv.submit(model, p))
+        tickets = []
+        t0 = time.perf_counter()
+        for (model, _, arrival), p in zip(stream, params):
+            delay = arrival - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            tickets.append(srv.submit(model, p))
+        lats, iters, ok = [], [], 0
+        for t in tickets:
+            r, lat = srv.poll(t)
+            lats.append(lat)
+            iters.append(r.iter)
+            ok += r.status == "OPTIMAL"
+        wall = time.perf_counter() - t0
+    rate = len(stream) / wall
+    lats = np.sort(np.asarray(lats))
+    line = {"metric": "solves/s", "value": rate, "unit": "solves/s", "n_gpus": 1, "steps": len(stream),
+            "warmup": 2, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded serving stream, seed 11)",
+            "config": {"workload": "serving stream of small SOCPs: n lognormal (median 400, 50..20000), "
+                                   "m = n/2, density 2-5%, 1-200 variable cones of 3-64, half with diagonal Q, "
+                                   "tolerance 1e-4 or 1e-6 per request",
+                       "slots": args.slots, "arrival_rate": args.rate or "saturation (all at t=0)"},
+            "latency_s": {"p50": float(np.percentile(lats, 50)), "p99": float(np.percentile(lats, 99)),
+                          "max": float(lats[-1])},
+            "optimal": ok, "mean_iterations": float(np.mean(iters)),
+            "one_at_a_time": {"value": seq_rate, "unit": "solves/s", "requests": nb,
+                              "how": "hpr_optimize per request, sequentially"},
+            "speedup_vs_one_at_a_time": rate / seq_rate}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -198,8 +257,17 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the instance (testing only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mode", default="iterate", choices=["iterate", "serve"],
+                    help="serve: the small-SOCP serving stream instead of the iteration benchmark")
+    ap.add_argument("--requests", type=int, default=400, help="serve: requests in the stream")
+    ap.add_argument("--slots", type=int, default=32, help="serve: concurrent solver slots")
+    ap.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrivals/s (0 = saturation)")
+    ap.add_argument("--baseline", type=int, default=60, help="serve: requests solved one at a time")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.mode == "serve":
+        run_serving(args)
+        return
 
     from hprsocp_b200 import instances
     if args.impl == "reference":

@@ -112,15 +112,15 @@ bool nonan_all(const double* v, int64_t n) {
 int put_vec(Ctx* c, double** d, const double* h, int64_t n) {
   HPR_TRY(dev_alloc_n(c, d, n));
   if (n > 0) {
-    if (h) HPR_CUDA(c, cudaMemcpy(*d, h, n * sizeof(double), cudaMemcpyHostToDevice));
-    else HPR_CUDA(c, cudaMemset(*d, 0, n * sizeof(double)));
+    if (h) HPR_CUDA(c, cudaMemcpyAsync(*d, h, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    else HPR_CUDA(c, cudaMemsetAsync(*d, 0, n * sizeof(double), c->stream));
   }
   return HPR_OK;
 }
 
 int zero_vec(Ctx* c, double** d, int64_t n) {
   HPR_TRY(dev_alloc_n(c, d, n));
-  HPR_CUDA(c, cudaMemset(*d, 0, std::max<int64_t>(n, 1) * sizeof(double)));
+  HPR_CUDA(c, cudaMemsetAsync(*d, 0, std::max<int64_t>(n, 1) * sizeof(double), c->stream));
   return HPR_OK;
 }
 
@@ -387,7 +387,8 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
       lamQ *= 1.05;
     } else {
       vector<double> qv(c->Q.nnz);
-      HPR_CUDA(c, cudaMemcpy(qv.data(), c->Q.val, c->Q.nnz * sizeof(double), cudaMemcpyDeviceToHost));
+      HPR_CUDA(c, cudaMemcpyAsync(qv.data(), c->Q.val, c->Q.nnz * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      HPR_CUDA(c, cudaStreamSynchronize(c->stream));
       lamQ = -kInf;
       for (double v : qv) lamQ = std::max(lamQ, v);
     }
@@ -735,8 +736,11 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
     vector<int32_t> cs(c->h_con_idx.begin(), c->h_con_idx.end()), vs(c->h_var_idx.begin(), c->h_var_idx.end());
     HPR_TRY(dev_alloc_n(c, &c->d_con_start, (int64_t)cs.size()));
     HPR_TRY(dev_alloc_n(c, &c->d_var_start, (int64_t)vs.size()));
-    HPR_CUDA(c, cudaMemcpy(c->d_con_start, cs.data(), cs.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-    HPR_CUDA(c, cudaMemcpy(c->d_var_start, vs.data(), vs.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    HPR_CUDA(c, cudaMemcpyAsync(c->d_con_start, cs.data(), cs.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                c->stream));
+    HPR_CUDA(c, cudaMemcpyAsync(c->d_var_start, vs.data(), vs.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                c->stream));
+    HPR_CUDA(c, cudaStreamSynchronize(c->stream));
   }
   // plans
   vector<int64_t> vcones = c->h_var_idx.size() > 1 ? c->h_var_idx : vector<int64_t>();

@@ -433,6 +433,14 @@ __global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineArgs a,
 // ---------------------------------------------------------------------------
 constexpr int kRedGrid = 592;  // 4 CTAs per SM on 148 SMs
 
+// CTAs of a plain reduction over n entries: a fixed function of n (so the
+// summation order, and the result, depend on n only), at most kRedGrid, and
+// small for small vectors so that concurrent contexts share the device.
+inline int red_grid(int64_t n) {
+  const int64_t g = (n + 8 * kThreads - 1) / (8 * kThreads);
+  return (int)(g < 1 ? 1 : (g > kRedGrid ? kRedGrid : g));
+}
+
 template <int NRED, unsigned MASK>
 __global__ void __launch_bounds__(kThreads) final_reduce_kernel(const double* __restrict__ slots, int nslots,
                                                                 double* __restrict__ out) {
@@ -477,8 +485,9 @@ inline int vec_reduce(Ctx* c, int64_t n, F f, int red_off) {
     HPR_CUDA(c, cudaMemsetAsync(c->d_red_out + red_off, 0, NRED * sizeof(double), c->stream));
     return HPR_OK;
   }
-  vec_reduce_kernel<NRED, MASK, F><<<kRedGrid, kThreads, 0, c->stream>>>(n, f, c->d_red);
-  final_reduce_kernel<NRED, MASK><<<1, kThreads, 0, c->stream>>>(c->d_red, kRedGrid, c->d_red_out + red_off);
+  const int g = red_grid(n);
+  vec_reduce_kernel<NRED, MASK, F><<<g, kThreads, 0, c->stream>>>(n, f, c->d_red);
+  final_reduce_kernel<NRED, MASK><<<1, kThreads, 0, c->stream>>>(c->d_red, g, c->d_red_out + red_off);
   c->launches += 2;
   HPR_CUDA(c, cudaGetLastError());
   return HPR_OK;

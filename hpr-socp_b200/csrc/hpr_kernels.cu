@@ -421,14 +421,17 @@ int upload_plan(Ctx* c, Plan& p) {
   HPR_TRY(dev_alloc_n(c, &p.d_partials, (int64_t)p.npartials));
   HPR_TRY(dev_alloc_n(c, &p.d_raw, p.nrows));
   HPR_TRY(dev_alloc_n(c, &p.d_ctr, 2));
-  if (nt) HPR_CUDA(c, cudaMemcpy(p.d_tasks, p.tasks.data(), nt * sizeof(Task), cudaMemcpyHostToDevice));
+  if (nt)
+    HPR_CUDA(c, cudaMemcpyAsync(p.d_tasks, p.tasks.data(), nt * sizeof(Task), cudaMemcpyHostToDevice, c->stream));
   if (!p.big.empty())
-    HPR_CUDA(c, cudaMemcpy(p.d_big, p.big.data(), p.big.size() * sizeof(BigCone), cudaMemcpyHostToDevice));
+    HPR_CUDA(c, cudaMemcpyAsync(p.d_big, p.big.data(), p.big.size() * sizeof(BigCone), cudaMemcpyHostToDevice,
+                                c->stream));
   if (!p.lng.empty())
-    HPR_CUDA(c, cudaMemcpy(p.d_lng, p.lng.data(), p.lng.size() * sizeof(LongRow), cudaMemcpyHostToDevice));
-  HPR_CUDA(c, cudaMemset(p.d_big_cnt, 0, std::max<size_t>(1, p.big.size()) * sizeof(int32_t)));
-  HPR_CUDA(c, cudaMemset(p.d_lng_cnt, 0, std::max<size_t>(1, p.lng.size()) * sizeof(int32_t)));
-  HPR_CUDA(c, cudaMemset(p.d_ctr, 0, 2 * sizeof(int32_t)));
+    HPR_CUDA(c, cudaMemcpyAsync(p.d_lng, p.lng.data(), p.lng.size() * sizeof(LongRow), cudaMemcpyHostToDevice,
+                                c->stream));
+  HPR_CUDA(c, cudaMemsetAsync(p.d_big_cnt, 0, std::max<size_t>(1, p.big.size()) * sizeof(int32_t), c->stream));
+  HPR_CUDA(c, cudaMemsetAsync(p.d_lng_cnt, 0, std::max<size_t>(1, p.lng.size()) * sizeof(int32_t), c->stream));
+  HPR_CUDA(c, cudaMemsetAsync(p.d_ctr, 0, 2 * sizeof(int32_t), c->stream));
   int64_t need = (int64_t)p.nslots() * kMaxRed;
   if (need > c->red_slots) {
     dev_free(c, c->d_red);
@@ -464,10 +467,11 @@ namespace {
 // SMs), computed once.
 template <class Epi, int PREC>
 int engine_grid(int* smem_bytes) {
-  static int grid = 0;
+  static std::once_flag once;
+  static int grid = 1;
   constexpr int dyn = kEngineSmem;
   *smem_bytes = dyn;
-  if (grid == 0) {
+  std::call_once(once, [] {
     auto k = engine_kernel<Epi, PREC>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     int per_sm = 0, dev = 0, sms = 0;
@@ -475,14 +479,17 @@ int engine_grid(int* smem_bytes) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     grid = std::max(1, per_sm) * std::max(1, sms);
-  }
+  });
   return grid;
 }
 
+// One warp per tile at most: a small problem occupies only the SMs it needs,
+// so other streams (other contexts of a serving process) run beside it.
 template <class Epi, int PREC>
 void launch_engine_prec(Ctx* c, int nt, const EngineArgs& a, const Epi& epi) {
   int dyn = 0;
-  int g = std::min(nt, engine_grid<Epi, PREC>(&dyn));
+  const int full = engine_grid<Epi, PREC>(&dyn);
+  const int g = std::max(1, std::min(full, (nt + kWarpsPerCta - 1) / kWarpsPerCta));
   engine_kernel<Epi, PREC><<<g, kEngineThreads, dyn, c->stream>>>(a, epi);
 }
 

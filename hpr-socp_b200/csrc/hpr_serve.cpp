@@ -1,0 +1,309 @@
+// hpr_serve.cpp — continuous-batching server for streams of small SOCPs.
+//
+// A server owns `slots` solver contexts on one device, each with its own
+// CUDA stream and host thread.  Submitted requests are deep-copied into a
+// FIFO; a slot takes the head of the queue as soon as it is free and the
+// request's estimated device memory fits the server's HBM budget, so
+// requests that arrive while others are on the GPU are admitted as slots and
+// memory free up, and the kernels of all running solves overlap on the
+// device (small problems launch only the CTAs their tiles need).  Each
+// request carries its own parameters, so each retires at its own tolerance.
+// A solve inside the server is exactly hpr_upload + hpr_solve on a private
+// context, so its result is bit-identical to solving it alone.
+//
+// The reference solves one model per `optimize` call (src/algorithm.jl:
+// 2538-2581) and its dataset runner loops over files one at a time
+// (src/utils/dataset.jl:4-122); this server is the B200 replacement for
+// that loop.  It uses only the public C ABI.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/hprsocp_b200.h"
+
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// A request's problem with every array owned by the server.
+struct OwnedCSR {
+  std::vector<int32_t> rp, ci;
+  std::vector<double> v;
+  hpr_csr view(const hpr_csr& s) const {
+    hpr_csr o = s;
+    o.rowptr = s.rowptr ? rp.data() : nullptr;
+    o.colind = s.colind ? ci.data() : nullptr;
+    o.values = s.values ? v.data() : nullptr;
+    return o;
+  }
+  void copy(const hpr_csr& s) {
+    if (s.rowptr && s.nrows >= 0) rp.assign(s.rowptr, s.rowptr + s.nrows + 1);
+    if (s.colind && s.nnz > 0) ci.assign(s.colind, s.colind + s.nnz);
+    if (s.values && s.nnz > 0) v.assign(s.values, s.values + s.nnz);
+  }
+};
+
+struct OwnedProblem {
+  hpr_problem p{};
+  OwnedCSR A, AT, Q, F;
+  std::vector<double> c, l, u, AL, AU, rhs, qd;
+  std::vector<int64_t> con, var;
+
+  static void vec(std::vector<double>& dst, const double* src, int64_t n) {
+    if (src && n > 0) dst.assign(src, src + n);
+  }
+  void copy(const hpr_problem& s) {
+    p = s;
+    A.copy(s.A);
+    AT.copy(s.AT);
+    Q.copy(s.Q);
+    F.copy(s.F);
+    vec(c, s.c, s.n);
+    vec(l, s.l, s.n);
+    vec(u, s.u, s.n);
+    vec(AL, s.AL, s.m);
+    vec(AU, s.AU, s.m);
+    vec(rhs, s.soc_rhs, s.m - s.m_lin);
+    vec(qd, s.q_diag, s.n);
+    if (s.soc_con_idx && s.n_soc_con_idx > 0) con.assign(s.soc_con_idx, s.soc_con_idx + s.n_soc_con_idx);
+    if (s.soc_var_idx && s.n_soc_var_idx > 0) var.assign(s.soc_var_idx, s.soc_var_idx + s.n_soc_var_idx);
+    p.A = A.view(s.A);
+    p.AT = AT.view(s.AT);
+    p.Q = Q.view(s.Q);
+    p.F = F.view(s.F);
+    auto ptr = [](const std::vector<double>& v, const double* orig) { return orig ? v.data() : nullptr; };
+    p.c = ptr(c, s.c);
+    p.l = ptr(l, s.l);
+    p.u = ptr(u, s.u);
+    p.AL = ptr(AL, s.AL);
+    p.AU = ptr(AU, s.AU);
+    p.soc_rhs = ptr(rhs, s.soc_rhs);
+    p.q_diag = ptr(qd, s.q_diag);
+    p.soc_con_idx = s.soc_con_idx ? con.data() : nullptr;
+    p.soc_var_idx = s.soc_var_idx ? var.data() : nullptr;
+  }
+};
+
+struct Request {
+  int64_t ticket = 0;
+  std::unique_ptr<OwnedProblem> prob;
+  hpr_params params{};
+  double t_submit = 0;
+  size_t est = 0;
+};
+
+struct Finished {
+  int rc = HPR_OK;
+  std::string err;
+  hpr_results res{};
+  std::vector<double> x, y, z, w;
+  double latency = 0;
+};
+
+// Device bytes one request needs: A and A' (value + index), the row
+// pointers, ~45 workspace vectors of length n or m, reduced-precision copies
+// and the tile plans, with a 25% margin and 1 MiB of fixed overhead.
+size_t estimate_bytes(const hpr_problem& p) {
+  const double nnz = (double)p.A.nnz, n = (double)p.n, m = (double)p.m;
+  double q = 0;
+  if (p.q_kind == HPR_Q_CSR) q = (double)p.Q.nnz * 24.0;
+  if (p.q_kind == HPR_Q_DIAG_LOWRANK) q = (double)p.F.nnz * 24.0 + 8.0 * n;
+  const double b = 2.0 * nnz * (12.0 + 6.0) + 8.0 * (n + m) + 8.0 * (45.0 * n + 30.0 * m) + q + 0.05 * nnz * 32.0;
+  return (size_t)(1.25 * b) + ((size_t)1 << 20);
+}
+
+}  // namespace
+
+struct hpr_server {
+  int device = 0;
+  size_t budget = 0, reserved = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Request> queue;
+  std::map<int64_t, Finished> done;
+  std::vector<std::thread> workers;
+  int64_t next_ticket = 1;
+  int64_t running = 0;
+  bool stop = false;
+  std::string err;
+
+  void worker(hpr_ctx* ctx) {
+    for (;;) {
+      Request r;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        // admission: the head of the queue enters once its memory fits
+        cv_work.wait(lk, [&] { return stop || (!queue.empty() && reserved + queue.front().est <= budget); });
+        if (stop) break;
+        r = std::move(queue.front());
+        queue.pop_front();
+        reserved += r.est;
+        ++running;
+      }
+      Finished f;
+      const int64_t n = r.prob->p.n, m = r.prob->p.m;
+      f.x.assign((size_t)n, 0.0);
+      f.y.assign((size_t)m, 0.0);
+      f.z.assign((size_t)n, 0.0);
+      f.w.assign((size_t)n, 0.0);
+      f.res.x = f.x.data();
+      f.res.y = f.y.data();
+      f.res.z = f.z.data();
+      f.res.w = f.w.data();
+      r.params.verbose = 0;
+      r.params.device_number = device;
+      f.rc = hpr_upload(ctx, &r.prob->p);
+      if (f.rc == HPR_OK) f.rc = hpr_solve(ctx, &r.params, &f.res);
+      if (f.rc != HPR_OK) f.err = hpr_last_error(ctx);
+      f.res.x = f.res.y = f.res.z = f.res.w = nullptr;
+      f.latency = now_s() - r.t_submit;
+      r.prob.reset();
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        reserved -= r.est;
+        --running;
+        done[r.ticket] = std::move(f);
+      }
+      cv_done.notify_all();
+      cv_work.notify_all();
+    }
+    hpr_destroy(ctx);
+  }
+};
+
+extern "C" {
+
+int hpr_serve_create(int device, int slots, size_t hbm_budget, hpr_server** out) {
+  if (!out || slots < 1 || slots > 1024) return HPR_E_BAD_INPUT;
+  *out = nullptr;
+  std::vector<hpr_ctx*> ctxs;
+  for (int i = 0; i < slots; ++i) {
+    hpr_ctx* c = nullptr;
+    int rc = hpr_create(device, 0, &c);
+    if (rc != HPR_OK) {
+      for (hpr_ctx* d : ctxs) hpr_destroy(d);
+      return rc;
+    }
+    ctxs.push_back(c);
+  }
+  hpr_server* s = new hpr_server();
+  s->device = device;
+  if (hbm_budget == 0) {
+    // 90% of what the device has free, as a single context would take
+    size_t fr = 0, tot = 0;
+    if (cudaSetDevice(device) != cudaSuccess || cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      for (hpr_ctx* d : ctxs) hpr_destroy(d);
+      delete s;
+      return HPR_E_CUDA;
+    }
+    hbm_budget = (size_t)(0.9 * (double)fr);
+  }
+  s->budget = hbm_budget;
+  for (hpr_ctx* c : ctxs) s->workers.emplace_back([s, c] { s->worker(c); });
+  *out = s;
+  return HPR_OK;
+}
+
+int hpr_serve_submit(hpr_server* s, const hpr_problem* prob, const hpr_params* params, int64_t* ticket) {
+  if (!s || !prob || !ticket) return HPR_E_BAD_INPUT;
+  if (prob->m < 0 || prob->n < 0 || prob->A.nnz < 0) return HPR_E_BAD_INPUT;
+  Request r;
+  r.est = estimate_bytes(*prob);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (r.est > s->budget) {
+      s->err = "request needs about " + std::to_string(r.est) + " bytes; the server's HBM budget is " +
+               std::to_string(s->budget);
+      return HPR_E_BUDGET;
+    }
+  }
+  r.prob.reset(new OwnedProblem());
+  r.prob->copy(*prob);
+  if (params) {
+    r.params = *params;
+  } else {
+    hpr_default_params(&r.params);
+  }
+  r.params.initial_x = nullptr;  // warm starts are not carried through the queue
+  r.params.initial_y = nullptr;
+  r.t_submit = now_s();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    r.ticket = s->next_ticket++;
+    *ticket = r.ticket;
+    s->queue.push_back(std::move(r));
+  }
+  s->cv_work.notify_all();
+  return HPR_OK;
+}
+
+int hpr_serve_poll(hpr_server* s, int64_t ticket, int wait_ms, hpr_results* res, double* latency_s) {
+  if (!s || ticket <= 0) return HPR_E_BAD_INPUT;
+  std::unique_lock<std::mutex> lk(s->mu);
+  if (ticket >= s->next_ticket) return HPR_E_BAD_INPUT;
+  auto ready = [&] { return s->done.count(ticket) > 0; };
+  if (wait_ms < 0) {
+    s->cv_done.wait(lk, ready);
+  } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), ready)) {
+    return HPR_E_TIMEOUT;
+  }
+  Finished f = std::move(s->done[ticket]);
+  s->done.erase(ticket);
+  lk.unlock();
+  if (latency_s) *latency_s = f.latency;
+  if (f.rc != HPR_OK) {
+    std::lock_guard<std::mutex> g(s->mu);
+    s->err = f.err;
+    return f.rc;
+  }
+  if (res) {
+    double *x = res->x, *y = res->y, *z = res->z, *w = res->w;
+    *res = f.res;
+    res->x = x;
+    res->y = y;
+    res->z = z;
+    res->w = w;
+    if (x) std::memcpy(x, f.x.data(), f.x.size() * sizeof(double));
+    if (y) std::memcpy(y, f.y.data(), f.y.size() * sizeof(double));
+    if (z) std::memcpy(z, f.z.data(), f.z.size() * sizeof(double));
+    if (w) std::memcpy(w, f.w.data(), f.w.size() * sizeof(double));
+  }
+  return HPR_OK;
+}
+
+int hpr_serve_stats(hpr_server* s, int64_t* queued, int64_t* running, size_t* reserved_bytes) {
+  if (!s) return HPR_E_BAD_INPUT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (queued) *queued = (int64_t)s->queue.size();
+  if (running) *running = s->running;
+  if (reserved_bytes) *reserved_bytes = s->reserved;
+  return HPR_OK;
+}
+
+const char* hpr_serve_last_error(hpr_server* s) { return s ? s->err.c_str() : "null server"; }
+
+int hpr_serve_destroy(hpr_server* s) {
+  if (!s) return HPR_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  for (std::thread& t : s->workers) t.join();
+  delete s;
+  return HPR_OK;
+}
+
+}  // extern "C"

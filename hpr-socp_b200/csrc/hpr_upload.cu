@@ -114,8 +114,9 @@ struct Scratch {
 int sort_rows_on_host(Ctx* c, DevCSR& M, const std::vector<int32_t>& rp) {
   std::vector<int32_t> ci(M.nnz);
   std::vector<double> v(M.nnz);
-  HPR_CUDA(c, cudaMemcpy(ci.data(), M.col, M.nnz * sizeof(int32_t), cudaMemcpyDeviceToHost));
-  HPR_CUDA(c, cudaMemcpy(v.data(), M.val, M.nnz * sizeof(double), cudaMemcpyDeviceToHost));
+  HPR_CUDA(c, cudaMemcpyAsync(ci.data(), M.col, M.nnz * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA(c, cudaMemcpyAsync(v.data(), M.val, M.nnz * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
   std::vector<std::pair<int32_t, double>> tmp;
   for (int64_t i = 0; i < M.nrows; ++i) {
     tmp.clear();
@@ -129,8 +130,9 @@ int sort_rows_on_host(Ctx* c, DevCSR& M, const std::vector<int32_t>& rp) {
       v[k] = tmp[k - rp[i]].second;
     }
   }
-  HPR_CUDA(c, cudaMemcpy(M.col, ci.data(), M.nnz * sizeof(int32_t), cudaMemcpyHostToDevice));
-  HPR_CUDA(c, cudaMemcpy(M.val, v.data(), M.nnz * sizeof(double), cudaMemcpyHostToDevice));
+  HPR_CUDA(c, cudaMemcpyAsync(M.col, ci.data(), M.nnz * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+  HPR_CUDA(c, cudaMemcpyAsync(M.val, v.data(), M.nnz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
   return HPR_OK;
 }
 

@@ -141,6 +141,12 @@ PROTOTYPES = {
                                C.POINTER(hpr_results)]),
     "hpr_last_iterate_ms": (C.c_int, [C.c_void_p, _dp, _lp]),
     "hpr_iteration_bytes": (C.c_int, [C.c_void_p, _dp]),
+    "hpr_serve_create": (C.c_int, [C.c_int, C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]),
+    "hpr_serve_submit": (C.c_int, [C.c_void_p, C.POINTER(hpr_problem), C.POINTER(hpr_params), _lp]),
+    "hpr_serve_poll": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.POINTER(hpr_results), _dp]),
+    "hpr_serve_stats": (C.c_int, [C.c_void_p, _lp, _lp, C.POINTER(C.c_size_t)]),
+    "hpr_serve_last_error": (C.c_char_p, [C.c_void_p]),
+    "hpr_serve_destroy": (C.c_int, [C.c_void_p]),
 }
 
 _LIB = None

@@ -206,3 +206,19 @@ def small_socp(seed: int, n: int = None, diag_q: bool = None) -> SOCPModel:
         model.Q = sp.diags(rng.uniform(0.0, 1.0, size=n)).tocsr()
         model.__post_init__()
     return model
+
+
+def serving_stream(seed: int, count: int, rate: float = 0.0):
+    """The serving workload: `count` small SOCPs (small_socp) with a per-request
+    tolerance of 1e-4 or 1e-6 (50/50) and Poisson arrival times at `rate`
+    requests/s (rate <= 0: everything arrives at t = 0, i.e. saturation).
+    Returns a list of (model, stoptol, arrival_s)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    t = 0.0
+    for k in range(count):
+        tol = 1e-4 if rng.integers(0, 2) == 0 else 1e-6
+        if rate > 0:
+            t += rng.exponential(1.0 / rate)
+        out.append((small_socp(int(rng.integers(0, 2**31 - 1))), tol, t))
+    return out

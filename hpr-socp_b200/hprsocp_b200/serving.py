@@ -1,0 +1,77 @@
+"""Continuous-batching server (hpr_serve_*): many small SOCPs solved
+concurrently on one device, each with its own parameters and tolerance."""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from .model import SOCPModel
+from .solver import HPRSOCP_parameters, HPRSOCP_results, results_from_c
+
+
+class Server:
+    """`slots` solver contexts on one device; requests are admitted while
+    their estimated device memory fits `hbm_budget` bytes (0 = 90% of free)."""
+
+    def __init__(self, slots: int = 16, device: int = 0, hbm_budget: int = 0):
+        self.lib = _abi.load_library()
+        h = C.c_void_p()
+        rc = self.lib.hpr_serve_create(device, slots, hbm_budget, C.byref(h))
+        if rc != _abi.HPR_OK:
+            raise _abi.HPRError(rc, self.lib.hpr_status_string(rc).decode())
+        self.h = h
+        self._shapes = {}
+
+    def _err(self, rc):
+        msg = self.lib.hpr_serve_last_error(self.h).decode() if self.h else ""
+        return _abi.HPRError(rc, f"{self.lib.hpr_status_string(rc).decode()}: {msg}")
+
+    def submit(self, model: SOCPModel, params: Optional[HPRSOCP_parameters] = None) -> int:
+        prob = model.to_c()
+        p = (params or HPRSOCP_parameters(verbose=False)).to_c()
+        t = C.c_int64()
+        rc = self.lib.hpr_serve_submit(self.h, C.byref(prob), C.byref(p), C.byref(t))
+        if rc != _abi.HPR_OK:
+            raise self._err(rc)
+        self._shapes[t.value] = (model.m, model.n)
+        return t.value
+
+    def poll(self, ticket: int, wait_ms: int = -1):
+        """(HPRSOCP_results, latency_s), or None if not finished within wait_ms."""
+        m, n = self._shapes[ticket]
+        x, y, z, w = np.zeros(n), np.zeros(m), np.zeros(n), np.zeros(n)
+        r = _abi.hpr_results()
+        r.x, r.y, r.z, r.w = _abi.dptr(x), _abi.dptr(y), _abi.dptr(z), _abi.dptr(w)
+        lat = C.c_double()
+        rc = self.lib.hpr_serve_poll(self.h, ticket, wait_ms, C.byref(r), C.byref(lat))
+        if rc == _abi.HPR_E_TIMEOUT:
+            return None
+        del self._shapes[ticket]
+        if rc != _abi.HPR_OK:
+            raise self._err(rc)
+        return results_from_c(r, x, y, z, w), lat.value
+
+    def stats(self):
+        q, run, res = C.c_int64(), C.c_int64(), C.c_size_t()
+        self.lib.hpr_serve_stats(self.h, C.byref(q), C.byref(run), C.byref(res))
+        return {"queued": q.value, "running": run.value, "reserved_bytes": res.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.hpr_serve_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

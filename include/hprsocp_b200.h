@@ -367,6 +367,41 @@ int hpr_last_iterate_ms(hpr_ctx* ctx, double* ms_total, int64_t* launches);
  * roofline numerator used by the benchmark).                               */
 int hpr_iteration_bytes(hpr_ctx* ctx, double* bytes_per_iter);
 
+/* ------------------------------------------------------------------------ */
+/* Serving: continuous batching of many small problems on one device.       */
+/* No single reference counterpart: it replaces calling optimize() once per */
+/* model in a loop (src/algorithm.jl:2538-2581, src/utils/dataset.jl:4-122). */
+/* ------------------------------------------------------------------------ */
+typedef struct hpr_server hpr_server;
+
+/* `slots` solver contexts (one stream and host thread each) on `device`;
+ * requests are admitted while their estimated device memory fits
+ * `hbm_budget` bytes (0 = 90% of the device's free memory).                */
+int hpr_serve_create(int device, int slots, size_t hbm_budget,
+                     hpr_server** out);
+
+/* Queue one problem with its own parameters (tolerance, limits, precision);
+ * the problem's arrays are copied, so the caller may free them on return.
+ * HPR_E_BUDGET if the request alone exceeds the server's budget.           */
+int hpr_serve_submit(hpr_server* srv, const hpr_problem* prob,
+                     const hpr_params* params, int64_t* ticket);
+
+/* Wait up to wait_ms (< 0: forever) for a ticket.  HPR_OK: `res` holds the
+ * result (x/y/z/w copied into the caller's buffers when non-NULL) and
+ * latency_s the time from submit to completion; the ticket is consumed.
+ * HPR_E_TIMEOUT: not finished yet.  Any other code: the solve's error
+ * (message in hpr_serve_last_error).                                        */
+int hpr_serve_poll(hpr_server* srv, int64_t ticket, int wait_ms,
+                   hpr_results* res, double* latency_s);
+
+int hpr_serve_stats(hpr_server* srv, int64_t* queued, int64_t* running,
+                    size_t* reserved_bytes);
+const char* hpr_serve_last_error(hpr_server* srv);
+
+/* Stops the slots after their current solves; queued requests are dropped.
+ * Poll every ticket you need before destroying the server.                 */
+int hpr_serve_destroy(hpr_server* srv);
+
 #ifdef __cplusplus
 }
 #endif

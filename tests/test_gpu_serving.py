@@ -1,0 +1,61 @@
+"""Continuous-batching server (hpr_serve_*): every request's result is the
+same alone and in the mix, each retires at its own tolerance, and admission
+respects the HBM budget."""
+import numpy as np
+import pytest
+
+from hprsocp_b200 import Context, HPRSOCP_parameters, _abi, instances
+from hprsocp_b200.serving import Server
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def stream():
+    return instances.serving_stream(7, 40)
+
+
+def _params(tol):
+    return HPRSOCP_parameters(verbose=False, stoptol=tol, max_iter=200000)
+
+
+def test_each_result_is_the_same_alone_and_in_the_mix(stream):
+    alone = []
+    for model, tol, _ in stream:
+        with Context(model) as ctx:
+            alone.append(ctx.solve(_params(tol)))
+    with Server(slots=16) as srv:
+        tickets = [srv.submit(model, _params(tol)) for model, tol, _ in stream]
+        mixed = [srv.poll(t)[0] for t in tickets]
+    for (model, tol, _), a, b in zip(stream, alone, mixed):
+        assert a.status == b.status == "OPTIMAL"
+        assert a.iter == b.iter
+        assert b.residuals <= tol
+        assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y) and np.array_equal(a.z, b.z)
+
+
+def test_each_request_retires_at_its_own_tolerance(stream):
+    model = stream[0][0]
+    with Server(slots=2) as srv:
+        t4 = srv.submit(model, _params(1e-4))
+        t6 = srv.submit(model, _params(1e-6))
+        r4, _ = srv.poll(t4)
+        r6, _ = srv.poll(t6)
+    assert r4.residuals <= 1e-4 and r6.residuals <= 1e-6
+    assert r4.iter <= r6.iter
+
+
+def test_admission_by_hbm_budget(stream):
+    """A small budget still serves every request that fits it; a request
+    larger than the whole budget is refused at submission."""
+    with Server(slots=4, hbm_budget=64 << 20) as srv:
+        small = [m for m, _, _ in stream if m.n <= 600][:4]
+        tickets = [srv.submit(m, _params(1e-4)) for m in small]
+        assert srv.stats()["reserved_bytes"] <= 64 << 20
+        for t in tickets:
+            r, lat = srv.poll(t)
+            assert r.status == "OPTIMAL" and lat > 0
+        big = instances.small_socp(3, n=12000)
+        with pytest.raises(_abi.HPRError) as e:
+            srv.submit(big, _params(1e-4))
+        assert e.value.code == _abi.HPR_E_BUDGET
