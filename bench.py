@@ -193,6 +193,8 @@ def run_serving(args):
     """Serving stream: small SOCPs (n lognormal, median 400) with per-request
     tolerances 1e-4 / 1e-6 through the continuous-batching server, against
     the same requests solved one at a time with hpr_optimize."""
+    # as many hardware work queues as slots can use (read at CUDA context creation)
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     import ctypes as C
     import numpy as np
     from hprsocp_b200 import HPRSOCP_parameters, _abi, instances

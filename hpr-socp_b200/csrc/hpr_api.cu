@@ -25,8 +25,9 @@ int dev_alloc(Ctx* c, void** p, size_t bytes) {
                    "HBM budget exceeded: need " + std::to_string(c->used + bytes) + " of " + std::to_string(c->budget));
   // stream-ordered pool allocation: memory released by an earlier context of
   // this process is reused instead of being mapped again
+  // (every use of the memory is ordered on c->stream, so no synchronisation
+  // is needed here)
   cudaError_t e = cudaMallocAsync(p, bytes, c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // usable from any stream from here on
   if (e != cudaSuccess) return set_err(c, HPR_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
   c->used += bytes;
   c->allocs[*p] = bytes;
@@ -403,7 +404,7 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
   HPR_TRY(update_q_factors(c));
   if (P->initial_x || P->initial_y) HPR_TRY(launch_initial_points(c, P->initial_x, P->initial_y));
   // small problems are launch-bound: replay captured partial iterations
-  if (c->A.nnz + c->n + c->m < (int64_t)4000000) HPR_TRY(capture_partial_graph(c, 8));
+  if (c->A.nnz + c->n + c->m < (int64_t)4000000 && !uses_fused_iterations(c)) HPR_TRY(capture_partial_graph(c, 8));
 
   RestartInfo R;
   R.best_sigma = c->sigma;
@@ -446,7 +447,8 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
         if (P->verbose)
           std::printf("switching the SpMV stream to FP64 at iteration %lld (KKT %.2e)\n", (long long)iter, kkt);
         HPR_TRY(apply_precision(c, HPR_PREC_FP64));
-        if (c->A.nnz + c->n + c->m < (int64_t)4000000) HPR_TRY(capture_partial_graph(c, 8));
+        if (c->A.nnz + c->n + c->m < (int64_t)4000000 && !uses_fused_iterations(c))
+          HPR_TRY(capture_partial_graph(c, 8));
       }
     }
     check_restart(R, iter, ci, c->sigma, rs.KKTx_and_gap_org_bar);

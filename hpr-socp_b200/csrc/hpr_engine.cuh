@@ -150,10 +150,23 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
   }
 }
 
-constexpr int kWarpsPerCta = 16;
+// Build-time tuning (defaults measured best on B200): warps per CTA, CTAs
+// per SM requested from the register allocator, tiles per atomic grab and
+// nonzeros per lane per gather round.
+#ifndef HPR_ENGINE_WARPS
+#define HPR_ENGINE_WARPS 8
+#endif
+#ifndef HPR_ENGINE_MINB
+#define HPR_ENGINE_MINB 3
+#endif
+#ifndef HPR_ENGINE_CHUNK
+#define HPR_ENGINE_CHUNK 2
+#endif
+constexpr int kWarpsPerCta = HPR_ENGINE_WARPS;
 constexpr int kEngineThreads = kWarpsPerCta * 32;
 constexpr int kGrab = 2;  // tiles taken per atomic
-constexpr int kChunk = 4; // elements per lane per gather round
+constexpr int kChunk = HPR_ENGINE_CHUNK;  // elements per lane per gather round
+constexpr bool kTwoRows = kRowCap > 32;   // a lane owns rows lane and lane + 32
 
 struct WarpSmem {
   double prod[kNnzTile];  // products, later per-cone norms
@@ -210,7 +223,10 @@ __device__ __forceinline__ bool arrive_big(const EngineArgs& a, int slot) {
   return __shfl_sync(0xffffffffu, last, 0) != 0;
 }
 
-template <class Epi, int PREC>
+// kCoherent: the gathered vector may have been written earlier in the same
+// launch (the fused multi-iteration kernel), so it is read through L2
+// instead of the read-only path.
+template <class Epi, int PREC, bool kCoherent = false>
 __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSmem& ws) {
   const int lane = threadIdx.x & 31;
   const Task t = a.pv.tasks[tix];
@@ -227,7 +243,7 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
       r0e = __ldg(a.M.rowptr + t.rb + lane + 1) - t.nzb;
       load_vals<Epi>(v0, epi, cone, t.rb + lane);
     }
-    if (lane + 32 < nrows) {
+    if (kTwoRows && lane + 32 < nrows) {
       r1b = __ldg(a.M.rowptr + t.rb + lane + 32) - t.nzb;
       r1e = __ldg(a.M.rowptr + t.rb + lane + 33) - t.nzb;
       load_vals<Epi>(v1, epi, cone, t.rb + lane + 32);
@@ -251,8 +267,10 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
     for (int k = 0; k < kChunk; ++k) {
       int e = c0 + lane + 32 * k;
       if (e < nnz) {
-        if constexpr (PREC == HPR_PREC_FP64) ws.prod[e] = vals[k] * __ldg(a.xin + cols[k]);
-        else ws.prod[e] = (double)((float)vals[k] * __ldg(a.xin32 + cols[k]));
+        if constexpr (PREC == HPR_PREC_FP64)
+          ws.prod[e] = vals[k] * (kCoherent ? __ldcg(a.xin + cols[k]) : __ldg(a.xin + cols[k]));
+        else
+          ws.prod[e] = (double)((float)vals[k] * (kCoherent ? __ldcg(a.xin32 + cols[k]) : __ldg(a.xin32 + cols[k])));
       }
     }
   }
@@ -314,7 +332,7 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
       long0 = true;
     }
   }
-  if (lane + 32 < nrows) {
+  if (kTwoRows && lane + 32 < nrows) {
     if (r1e - r1b <= kSerialMax) {
       double s = 0.0;
       for (int k = r1b; k < r1e; ++k) s = s + ws.prod[k];
@@ -324,7 +342,7 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
     }
   }
   {
-    unsigned m0 = __ballot_sync(0xffffffffu, long0), m1 = __ballot_sync(0xffffffffu, long1);
+    unsigned m0 = __ballot_sync(0xffffffffu, long0), m1 = kTwoRows ? __ballot_sync(0xffffffffu, long1) : 0u;
     while (m0 | m1) {
       int src_lane, rr;
       if (m0) {
@@ -349,7 +367,7 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
   // ---- 3. epilogue
   if (!cone) {
     if (lane < nrows) epi.linear(t.rb + lane, ws.acc[lane], v0, red);
-    if (lane + 32 < nrows) epi.linear(t.rb + lane + 32, ws.acc[lane + 32], v1, red);
+    if (kTwoRows && lane + 32 < nrows) epi.linear(t.rb + lane + 32, ws.acc[lane + 32], v1, red);
     if constexpr (Epi::kNRed > 0) {
       if (t.kind == TASK_CONE_PART && lane == 0) {
         double* dst = a.red_slots + (int64_t)(a.pv.ntasks + t.group) * kMaxRed;
@@ -358,14 +376,15 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
     }
   } else if (t.kind == TASK_CONE_PART) {
     if (lane < nrows) a.pv.raw[t.rb + lane] = epi.cone_raw(t.rb + lane, ws.acc[lane], v0, red);
-    if (lane + 32 < nrows) a.pv.raw[t.rb + lane + 32] = epi.cone_raw(t.rb + lane + 32, ws.acc[lane + 32], v1, red);
+    if (kTwoRows && lane + 32 < nrows)
+      a.pv.raw[t.rb + lane + 32] = epi.cone_raw(t.rb + lane + 32, ws.acc[lane + 32], v1, red);
     if (arrive_big(a, t.group)) finalize_big_cone(a, epi, t.group);
   } else {
     // whole small cones: raw values in place, one lane per cone for the
     // norm (ascending order, like the reference), one lane per row for the
     // projection.
     if (lane < nrows) ws.acc[lane] = epi.cone_raw(t.rb + lane, ws.acc[lane], v0, red);
-    if (lane + 32 < nrows) ws.acc[lane + 32] = epi.cone_raw(t.rb + lane + 32, ws.acc[lane + 32], v1, red);
+    if (kTwoRows && lane + 32 < nrows) ws.acc[lane + 32] = epi.cone_raw(t.rb + lane + 32, ws.acc[lane + 32], v1, red);
     __syncwarp();
     double* ns = ws.prod;  // products are dead
     for (int k = lane; k < t.ncones; k += 32) {
@@ -381,7 +400,7 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
       int h = ws.aux[lane];
       epi.cone_apply(t.rb + lane, ws.acc[lane], ws.acc[h], ns[h], lane == h, v0, red);
     }
-    if (lane + 32 < nrows) {
+    if (kTwoRows && lane + 32 < nrows) {
       int r = lane + 32, h = ws.aux[r];
       epi.cone_apply(t.rb + r, ws.acc[r], ws.acc[h], ns[h], r == h, v1, red);
     }
@@ -401,7 +420,7 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
 constexpr int kEngineSmem = kWarpsPerCta * (int)sizeof(WarpSmem);
 
 template <class Epi, int PREC>
-__global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineArgs a, Epi epi) {
+__global__ void __launch_bounds__(kEngineThreads, HPR_ENGINE_MINB) engine_kernel(EngineArgs a, Epi epi) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem* s_ws = reinterpret_cast<WarpSmem*>(smem_raw);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;

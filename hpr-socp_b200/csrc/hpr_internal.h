@@ -25,9 +25,13 @@ namespace hpr {
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;
 constexpr int kNnzTile = 512;
-constexpr int kRowCap = 64;
+#ifndef HPR_ENGINE_ROWCAP
+#define HPR_ENGINE_ROWCAP 32
+#endif
+constexpr int kRowCap = HPR_ENGINE_ROWCAP;  // 32 (one row per lane) or 64 (two)
+static_assert(kRowCap == 32 || kRowCap == 64, "one or two rows per lane");
 constexpr int kSerialMax = 64;      // rows longer than this use a warp reduction
-constexpr int kSmallConeMax = 64;   // larger cones are split over several tiles
+constexpr int kSmallConeMax = kRowCap;  // larger cones are split over several tiles
 constexpr int kMaxRed = 8;          // reduction lanes per engine launch
 
 enum TaskKind : int16_t {
@@ -211,6 +215,8 @@ int upload_plan(Ctx* c, Plan& p);
 PlanView view_of(const Plan& p, const int32_t* cone_start);
 int launch_iteration(Ctx* c, bool full);
 int run_iterations(Ctx* c, int64_t k, bool full_last);
+// true when run_iterations uses the single-CTA multi-iteration kernel
+bool uses_fused_iterations(const Ctx* c);
 int launch_residuals(Ctx* c, bool include_bounds, hpr_residuals* out);
 int launch_residuals_noalloc(Ctx* c, bool include_bounds, hpr_residuals* out);
 int launch_mnorm(Ctx* c, double* out);

@@ -603,10 +603,22 @@ int update_q_factors(Ctx* c) {
   });
 }
 
-int launch_iteration(Ctx* c, bool full) {
-  const bool fp32 = c->precision != HPR_PREC_FP64;
+namespace {
+
+// Epilogues of one HPR iteration (no-Q: EpiX, EpiY; Q: EpiQX, EpiQT, EpiY,
+// EpiW2), set up from the context's workspace.
+struct IterEpis {
   EpiY ey{};
+  EpiX ex{};
+  EpiQX eq{};
+  EpiQT et{};
+  EpiW2 e2{};
+};
+
+void make_iter_epis(Ctx* c, bool full, IterEpis& E) {
+  const bool fp32 = c->precision != HPR_PREC_FP64;
   if (c->m > 0) {
+    EpiY& ey = E.ey;
     const double* ysrc[4] = {c->y, c->last_y, c->AL, c->AU};
     const double* ycone[4] = {c->y, c->last_y, c->soc_rhs_full, nullptr};
     for (int k = 0; k < 4; ++k) {
@@ -622,8 +634,7 @@ int launch_iteration(Ctx* c, bool full) {
     ey.ybar_always = c->has_q ? 1 : 0;
   }
   if (!c->has_q) {
-    // main_update_noQ_soc_gpu! (algorithm.jl:2302-2309)
-    EpiX ex{};
+    EpiX& ex = E.ex;
     const double* xsrc[5] = {c->x, c->last_x, c->c, c->l, c->u};
     for (int k = 0; k < 5; ++k) {
       ex.lin_src[k] = xsrc[k];
@@ -636,16 +647,10 @@ int launch_iteration(Ctx* c, bool full) {
     ex.dx = c->dx;
     ex.x_hat32 = fp32 ? c->g32_n : nullptr;
     ex.full = full ? 1 : 0;
-    HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y, fp32 ? c->g32_m : nullptr, ex, c->m == 0,
-                          false, 0));
-    if (c->m > 0)
-      HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->x_hat, fp32 ? c->g32_n : nullptr, ey, true, false,
-                            0));
-    return HPR_OK;
+    return;
   }
-  // Q path: zxw1, y, w2 (algorithm.jl:2291-2295)
   const bool lowrank = c->q_kind == HPR_Q_DIAG_LOWRANK;
-  EpiQX eq{};
+  EpiQX& eq = E.eq;
   const double* qsrc[7] = {c->x, c->last_x, c->c, c->ATy, c->w, c->l, c->u};
   for (int k = 0; k < 7; ++k) {
     eq.lin_src[k] = qsrc[k];
@@ -663,29 +668,13 @@ int launch_iteration(Ctx* c, bool full) {
   eq.Qw = c->Qw;
   eq.full = full ? 1 : 0;
   eq.diag = c->Q_is_diag ? 1 : 0;
-  if (lowrank) {
-    HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, c->w, nullptr, plain(c->ftmp), false, false, 0));
-    HPR_TRY(engine_launch(c, c->FT, c->planQ, c->d_var_start, c->ftmp, nullptr, eq, false, false, 0));
-  } else {
-    HPR_TRY(engine_launch(c, c->Q, c->planQ, c->d_var_start, c->w, nullptr, eq, false, false, 0));
-  }
-  if (c->m > 0) {
-    EpiQT et{};
-    const double* tsrc[3] = {c->x_hat, c->Qw, c->w_bar};
-    for (int k = 0; k < 3; ++k) et.lin_src[k] = et.cone_src[k] = tsrc[k];
-    et.qdiag = lowrank ? c->qdiag : nullptr;
-    et.tempv = c->tempv;
-    et.tempv32 = fp32 ? c->g32_n : nullptr;
-    if (lowrank) {
-      HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, c->w_bar, nullptr, plain(c->ftmp2), false, false, 0));
-      HPR_TRY(engine_launch(c, c->FT, c->planQ, c->d_var_start, c->ftmp2, nullptr, et, false, false, 0));
-    } else {
-      HPR_TRY(engine_launch(c, c->Q, c->planQ, c->d_var_start, c->w_bar, nullptr, et, false, false, 0));
-    }
-    HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->tempv, fp32 ? c->g32_n : nullptr, ey, false, false,
-                          0));
-  }
-  EpiW2 e2{};
+  EpiQT& et = E.et;
+  const double* tsrc[3] = {c->x_hat, c->Qw, c->w_bar};
+  for (int k = 0; k < 3; ++k) et.lin_src[k] = et.cone_src[k] = tsrc[k];
+  et.qdiag = lowrank ? c->qdiag : nullptr;
+  et.tempv = c->tempv;
+  et.tempv32 = fp32 ? c->g32_n : nullptr;
+  EpiW2& e2 = E.e2;
   const double* wsrc[5] = {c->w, c->w_bar, c->ATy, c->last_w, c->last_ATy};
   for (int k = 0; k < 5; ++k) e2.lin_src[k] = e2.cone_src[k] = wsrc[k];
   e2.fact = c->fact;
@@ -697,13 +686,180 @@ int launch_iteration(Ctx* c, bool full) {
   e2.atdy = c->ATdy;
   e2.full = full ? 1 : 0;
   e2.diag = c->Q_is_diag ? 1 : 0;
-  return engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, e2, true, false, 0);
 }
+
+}  // namespace
+
+int launch_iteration(Ctx* c, bool full) {
+  const bool fp32 = c->precision != HPR_PREC_FP64;
+  IterEpis E;
+  make_iter_epis(c, full, E);
+  if (!c->has_q) {
+    // main_update_noQ_soc_gpu! (algorithm.jl:2302-2309)
+    HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, c->y, fp32 ? c->g32_m : nullptr, E.ex, c->m == 0,
+                          false, 0));
+    if (c->m > 0)
+      HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->x_hat, fp32 ? c->g32_n : nullptr, E.ey, true, false,
+                            0));
+    return HPR_OK;
+  }
+  // Q path: zxw1, y, w2 (algorithm.jl:2291-2295)
+  const bool lowrank = c->q_kind == HPR_Q_DIAG_LOWRANK;
+  if (lowrank) {
+    HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, c->w, nullptr, plain(c->ftmp), false, false, 0));
+    HPR_TRY(engine_launch(c, c->FT, c->planQ, c->d_var_start, c->ftmp, nullptr, E.eq, false, false, 0));
+  } else {
+    HPR_TRY(engine_launch(c, c->Q, c->planQ, c->d_var_start, c->w, nullptr, E.eq, false, false, 0));
+  }
+  if (c->m > 0) {
+    if (lowrank) {
+      HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, c->w_bar, nullptr, plain(c->ftmp2), false, false, 0));
+      HPR_TRY(engine_launch(c, c->FT, c->planQ, c->d_var_start, c->ftmp2, nullptr, E.et, false, false, 0));
+    } else {
+      HPR_TRY(engine_launch(c, c->Q, c->planQ, c->d_var_start, c->w_bar, nullptr, E.et, false, false, 0));
+    }
+    HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->tempv, fp32 ? c->g32_n : nullptr, E.ey, false, false,
+                          0));
+  }
+  return engine_launch(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, E.e2, true, false, 0);
+}
+
+// ---------------------------------------------------------------------------
+// Fused multi-iteration kernel for small problems.
+//
+// When every matrix side fits a few tiles per warp, one CTA runs k whole
+// iterations in a single launch: its warps split each half-step's tiles
+// statically, a CTA barrier separates the half-steps (the next half-step
+// gathers what the previous one wrote, through L2), and thread 0 advances
+// the Halpern counter after each iteration.  This replaces 2-4 launches per
+// iteration by one launch per batch, which is what bounds small solves and
+// lets many of them share the device.  Arithmetic and order per row are
+// those of the engine, so results are identical to the unfused path.
+// ---------------------------------------------------------------------------
+#ifndef HPR_FUSED_MAX_TILES
+#define HPR_FUSED_MAX_TILES (4 * kWarpsPerCta)
+#endif
+constexpr int kFusedMaxTiles = HPR_FUSED_MAX_TILES;
+
+namespace {
+
+template <class E>
+struct FStage {
+  EngineArgs a;
+  E part, full;
+  int on;
+};
+
+template <class E, int PREC>
+__device__ __forceinline__ void fused_stage(const FStage<E>& s, bool last, WarpSmem& ws) {
+  if (!s.on) return;
+  E e = last ? s.full : s.part;
+  e.setup(s.a.st);
+  for (int t = threadIdx.x >> 5; t < s.a.pv.ntasks; t += kWarpsPerCta) process_warp_tile<E, PREC, true>(s.a, e, t, ws);
+  __syncthreads();
+}
+
+// Stages run in order each iteration; `full_last` selects the full
+// epilogues on the last iteration.
+template <class E0, class E1, class E2, class E3, int PREC>
+__global__ void __launch_bounds__(kEngineThreads, 1)
+    fused_kernel(FStage<E0> s0, FStage<E1> s1, FStage<E2> s2, FStage<E3> s3, DevState* st, int iters, int full_last) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmem& ws = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
+  for (int it = 0; it < iters; ++it) {
+    const bool last = full_last && it + 1 == iters;
+    fused_stage<E0, PREC>(s0, last, ws);
+    fused_stage<E1, PREC>(s1, last, ws);
+    fused_stage<E2, PREC>(s2, last, ws);
+    fused_stage<E3, PREC>(s3, last, ws);
+    if (threadIdx.x == 0) st->inner = st->inner + 1;
+    __syncthreads();
+  }
+}
+
+template <class E>
+FStage<E> fstage(Ctx* c, const DevCSR& M, const Plan& p, const int32_t* cs, const double* xin, const float* xin32,
+                 const E& part, const E& full, bool on) {
+  FStage<E> s;
+  s.a.M = M;
+  s.a.xin = xin;
+  s.a.xin32 = xin32;
+  s.a.pv = view_of(p, cs);
+  s.a.st = c->d_state;
+  s.a.red_slots = nullptr;
+  s.a.bump_inner = 0;
+  s.part = part;
+  s.full = full;
+  s.on = on ? 1 : 0;
+  return s;
+}
+
+template <class E0, class E1, class E2, class E3>
+int launch_fused_prec(Ctx* c, const FStage<E0>& s0, const FStage<E1>& s1, const FStage<E2>& s2, const FStage<E3>& s3,
+                      int iters, int full_last) {
+  const int prec = c->precision;
+  auto go = [&](auto kernel) {
+    kernel<<<1, kEngineThreads, kEngineSmem, c->stream>>>(s0, s1, s2, s3, c->d_state, iters, full_last);
+  };
+  if (prec == HPR_PREC_FP32 && s0.a.M.val32) go(fused_kernel<E0, E1, E2, E3, HPR_PREC_FP32>);
+  else if (prec == HPR_PREC_BF16 && s0.a.M.val16) go(fused_kernel<E0, E1, E2, E3, HPR_PREC_BF16>);
+  else go(fused_kernel<E0, E1, E2, E3, HPR_PREC_FP64>);
+  c->launches++;
+  HPR_CUDA(c, cudaGetLastError());
+  return HPR_OK;
+}
+
+bool fused_eligible(const Ctx* c) {
+  if (c->q_kind == HPR_Q_DIAG_LOWRANK) return false;
+  auto fits = [](const Plan& p) { return (int64_t)p.tasks.size() <= kFusedMaxTiles; };
+  if (!fits(c->planX) || !fits(c->planY)) return false;
+  // with Q the reduced-precision streams apply to A only; keep those unfused
+  if (c->has_q && (!fits(c->planQ) || c->precision != HPR_PREC_FP64)) return false;
+  return kEngineSmem <= 48 * 1024;
+}
+
+// k iterations (the last one full when full_last) in one launch.
+int launch_fused(Ctx* c, int64_t k, bool full_last) {
+  const bool fp32 = c->precision != HPR_PREC_FP64;
+  IterEpis P, F;
+  make_iter_epis(c, false, P);
+  make_iter_epis(c, true, F);
+  const bool hy = c->m > 0;
+  for (int64_t done = 0; done < k;) {
+    const int n = (int)std::min<int64_t>(k - done, 1 << 20);
+    const int fl = (full_last && done + n == k) ? 1 : 0;
+    if (!c->has_q) {
+      auto sx = fstage(c, c->AT, c->planX, c->d_var_start, c->y, fp32 ? c->g32_m : nullptr, P.ex, F.ex, true);
+      auto sy = fstage(c, c->A, c->planY, c->d_con_start, c->x_hat, fp32 ? c->g32_n : nullptr, P.ey, F.ey, hy);
+      auto off = fstage(c, c->A, c->planY, c->d_con_start, c->x_hat, nullptr, P.ey, F.ey, false);
+      HPR_TRY(launch_fused_prec(c, sx, sy, off, off, n, fl));
+    } else {
+      auto sq = fstage(c, c->Q, c->planQ, c->d_var_start, c->w, nullptr, P.eq, F.eq, true);
+      auto st = fstage(c, c->Q, c->planQ, c->d_var_start, c->w_bar, nullptr, P.et, F.et, hy);
+      auto sy = fstage(c, c->A, c->planY, c->d_con_start, c->tempv, fp32 ? c->g32_n : nullptr, P.ey, F.ey, hy);
+      auto sw = fstage(c, c->AT, c->planX, c->d_var_start, c->y_bar, nullptr, P.e2, F.e2, true);
+      HPR_TRY(launch_fused_prec(c, sq, st, sy, sw, n, fl));
+    }
+    done += n;
+  }
+  return HPR_OK;
+}
+
+}  // namespace
+
+bool uses_fused_iterations(const Ctx* c) { return fused_eligible(c); }
 
 int run_iterations(Ctx* c, int64_t k, bool full_last) {
   if (k <= 0) return HPR_OK;
   int64_t l0 = c->launches;
   HPR_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+  if (fused_eligible(c)) {
+    HPR_TRY(launch_fused(c, k, full_last));
+    HPR_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    c->inner += k;
+    c->last_launches = c->launches - l0;
+    return HPR_OK;
+  }
   int64_t partial = full_last ? k - 1 : k;
   int64_t done = 0;
   // replay the captured partial-iteration graph where it fits
@@ -1026,6 +1182,75 @@ void power_start_vector(std::vector<double>& z, uint64_t seed) {
 }
 
 namespace {
+
+// The power iteration on lambda_max(AA') for small problems, entirely inside
+// one CTA: the same steps as power_generic (q = z/|z|, z = A (A' q),
+// lambda = <q, z>, err = |z - lambda q| / (|z| + lambda)) with the
+// convergence test on the device, so no host round trip per iteration.
+// out[0] = lambda, out[1] = iterations run.
+__global__ void __launch_bounds__(kEngineThreads, 1)
+    fused_power_kernel(FStage<EpiPlain> s_at, FStage<EpiPlain> s_a, double* z, double* q, int64_t m, int maxit,
+                       double tol, double* out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmem& ws = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
+  __shared__ double s_red[kMaxRed][kThreads / 32];
+  __shared__ double s_b[4];
+  double lambda = 1.0;
+  int it = 0;
+  for (; it < maxit; ++it) {
+    Red r;
+    red_init<1, 0>(r);
+    for (int64_t i = threadIdx.x; i < m; i += blockDim.x) r.v[0] = r.v[0] + z[i] * z[i];
+    block_reduce<1, 0>(r, s_red);
+    if (threadIdx.x == 0) s_b[0] = sqrt(r.v[0]);
+    __syncthreads();
+    const double nz = s_b[0];
+    for (int64_t i = threadIdx.x; i < m; i += blockDim.x) q[i] = z[i] / nz;
+    __syncthreads();
+    fused_stage<EpiPlain, HPR_PREC_FP64>(s_at, false, ws);  // ptq = A' q
+    fused_stage<EpiPlain, HPR_PREC_FP64>(s_a, false, ws);   // z = A ptq
+    red_init<1, 0>(r);
+    for (int64_t i = threadIdx.x; i < m; i += blockDim.x) r.v[0] = r.v[0] + q[i] * z[i];
+    block_reduce<1, 0>(r, s_red);
+    if (threadIdx.x == 0) s_b[1] = r.v[0];
+    __syncthreads();
+    lambda = s_b[1];
+    Red r2;
+    red_init<2, 0>(r2);
+    for (int64_t i = threadIdx.x; i < m; i += blockDim.x) {
+      const double qi = z[i] - lambda * q[i];
+      q[i] = qi;
+      r2.v[0] = r2.v[0] + qi * qi;
+      r2.v[1] = r2.v[1] + z[i] * z[i];
+    }
+    block_reduce<2, 0>(r2, s_red);
+    if (threadIdx.x == 0) s_b[2] = sqrt(r2.v[0]) / (sqrt(r2.v[1]) + lambda);
+    __syncthreads();
+    if (s_b[2] < tol) break;
+  }
+  if (threadIdx.x == 0) {
+    out[0] = lambda;
+    out[1] = (double)it;
+  }
+}
+
+int power_fused_A(Ctx* c, int maxit, double tol, double* lam) {
+  std::vector<double> hz(c->m);
+  power_start_vector(hz, 1);
+  HPR_CUDA(c, cudaMemcpyAsync(c->pz, hz.data(), c->m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  auto sat = fstage(c, c->AT, c->planX, c->d_var_start, c->pq, nullptr, plain(c->ptq), plain(c->ptq), true);
+  auto sa = fstage(c, c->A, c->planY, c->d_con_start, c->ptq, nullptr, plain(c->pz), plain(c->pz), true);
+  fused_power_kernel<<<1, kEngineThreads, kEngineSmem, c->stream>>>(sat, sa, c->pz, c->pq, c->m, maxit, tol,
+                                                                     c->d_red_out + 40);
+  c->launches++;
+  HPR_CUDA(c, cudaGetLastError());
+  HPR_CUDA(c, cudaMemcpyAsync(c->h_red_out + 40, c->d_red_out + 40, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                              c->stream));
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  *lam = c->h_red_out[40];
+  return HPR_OK;
+}
+
 int power_generic(Ctx* c, int64_t len, bool isA, int maxit, double tol, double* lam) {
   std::vector<double> hz(len);
   power_start_vector(hz, 1);
@@ -1067,6 +1292,8 @@ int launch_power_A(Ctx* c, int maxit, double tol, double* lam) {
     *lam = 0.0;
     return HPR_OK;
   }
+  auto small = [](const Plan& p) { return (int64_t)p.tasks.size() <= kFusedMaxTiles; };
+  if (small(c->planX) && small(c->planY) && kEngineSmem <= 48 * 1024) return power_fused_A(c, maxit, tol, lam);
   return power_generic(c, c->m, true, maxit, tol, lam);
 }
 

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -188,6 +189,11 @@ extern "C" {
 int hpr_serve_create(int device, int slots, size_t hbm_budget, hpr_server** out) {
   if (!out || slots < 1 || slots > 1024) return HPR_E_BAD_INPUT;
   *out = nullptr;
+  // The slots' streams run concurrently only if the device context has as
+  // many hardware work queues; CUDA's default is 8.  This takes effect when
+  // it is set before the process creates its CUDA context (an existing
+  // setting is kept).
+  setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
   std::vector<hpr_ctx*> ctxs;
   for (int i = 0; i < slots; ++i) {
     hpr_ctx* c = nullptr;

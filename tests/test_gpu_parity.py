@@ -21,8 +21,11 @@ VECS = ["x", "x_hat", "x_bar", "z_bar", "y", "y_bar", "s", "dx", "dy"]
 
 @pytest.fixture(scope="module")
 def models():
+    # small_* fit the single-CTA multi-iteration kernel (a few tiles per side)
     return {"config0": instances.config0(0), "stress": stress_model(5),
-            "config1_small": instances.config1(11, scale=0.004)}
+            "config1_small": instances.config1(11, scale=0.004),
+            "small_noq": instances.small_socp(21, n=300, diag_q=False),
+            "small_q": instances.small_socp(22, n=300, diag_q=True)}
 
 
 def _pair(model):
@@ -59,7 +62,7 @@ def test_scaling_parity(models, name):
         assert rel_err(a[fin], b[fin]) <= SCALE_TOL, v
 
 
-@pytest.mark.parametrize("name", ["config0", "stress", "config1_small"])
+@pytest.mark.parametrize("name", ["config0", "stress", "config1_small", "small_noq", "small_q"])
 @pytest.mark.parametrize("K", [1, 150, 1000])
 def test_iterate_parity(models, name, K):
     o, g = _pair(models[name])
@@ -115,8 +118,9 @@ def test_restart_parity(models):
         assert rel_err(g.get(v), o.get(v)) <= ITER_TOL, v
 
 
-def test_power_iteration_parity(models):
-    o, g = _pair(models["stress"])
+@pytest.mark.parametrize("name", ["stress", "small_noq", "small_q"])
+def test_power_iteration_parity(models, name):
+    o, g = _pair(models[name])
     p = HPRSOCP_parameters(verbose=False)
     o.scale(p)
     g.scale(p)
@@ -142,3 +146,14 @@ def test_solve_is_deterministic(models):
     r2 = Context(models["stress"]).solve(p)
     assert r1.iter == r2.iter
     assert np.array_equal(r1.x, r2.x) and np.array_equal(r1.y, r2.y)
+
+
+@pytest.mark.parametrize("name", ["small_noq", "small_q"])
+def test_solve_parity_small(models, name):
+    p = HPRSOCP_parameters(verbose=False, stoptol=1e-6, max_iter=100000)
+    o, g = _pair(models[name])
+    ro = o.solve(p)
+    rg = g.solve(p)
+    assert ro.status == rg.status == "OPTIMAL"
+    assert abs(rg.primal_obj - ro.primal_obj) <= 1e-6 * max(1.0, abs(ro.primal_obj))
+    assert abs(rg.iter - ro.iter) <= max(10, ro.iter // 20), (rg.iter, ro.iter)
