@@ -250,6 +250,41 @@ def run_serving(args):
     print(json.dumps(line))
 
 
+def run_tts(args):
+    """Time to solution at 1e-6 KKT on the benchmark SOCP with the plain FP64
+    stream and the reduced-precision streams (FP32 values and gathers; BF16
+    values with FP32 accumulation), each with the FP64 finish, and the error
+    of each result against the FP64 solution."""
+    import numpy as np
+    from hprsocp_b200 import Context, HPRSOCP_parameters, instances
+    model = instances.config1(1, scale=args.scale)
+    out = {}
+    ref = None
+    for prec in ("fp64", "fp32", "bf16"):
+        p = HPRSOCP_parameters(verbose=False, stoptol=1e-6, max_iter=200000, time_limit=600, precision=prec)
+        with Context(model) as ctx:
+            t0 = time.perf_counter()
+            r = ctx.solve(p)
+            wall = time.perf_counter() - t0
+        d = {"status": r.status, "iterations": r.iter, "solve_s": r.time, "wall_s": wall, "kkt": r.residuals,
+             "primal_obj": r.primal_obj}
+        if ref is None:
+            ref = r
+        else:
+            d["x_rel_err"] = float(np.max(np.abs(r.x - ref.x)) / max(1.0, np.max(np.abs(ref.x))))
+            d["y_rel_err"] = float(np.max(np.abs(r.y - ref.y)) / max(1.0, np.max(np.abs(ref.y))))
+            d["obj_rel_err"] = abs(r.primal_obj - ref.primal_obj) / max(1.0, abs(ref.primal_obj))
+            d["speedup_vs_fp64"] = ref.time / r.time
+        out[prec] = d
+    line = {"metric": "time to 1e-6 KKT", "value": out["fp32"]["solve_s"], "unit": "s", "n_gpus": 1, "steps": 1,
+            "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32/bf16",
+            "data": "synthetic (seeded generator, seed 1)",
+            "config": {"workload": WORKLOAD, "scale": args.scale,
+                       "what": "solve() to stoptol 1e-6 per SpMV precision; residuals, restart and sigma in FP64"},
+            "runs": out}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -259,8 +294,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the instance (testing only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", default="iterate", choices=["iterate", "serve"],
-                    help="serve: the small-SOCP serving stream instead of the iteration benchmark")
+    ap.add_argument("--mode", default="iterate", choices=["iterate", "serve", "tts"],
+                    help="serve: the small-SOCP serving stream; tts: time to 1e-6 per SpMV precision")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests in the stream")
     ap.add_argument("--slots", type=int, default=32, help="serve: concurrent solver slots")
     ap.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrivals/s (0 = saturation)")
@@ -269,6 +304,9 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.mode == "serve":
         run_serving(args)
+        return
+    if args.mode == "tts":
+        run_tts(args)
         return
 
     from hprsocp_b200 import instances

@@ -162,6 +162,9 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #ifndef HPR_ENGINE_CHUNK
 #define HPR_ENGINE_CHUNK 2
 #endif
+#ifndef HPR_ENGINE_PIPE
+#define HPR_ENGINE_PIPE 1  // next round's col/val requested before this round's gathers
+#endif
 constexpr int kWarpsPerCta = HPR_ENGINE_WARPS;
 constexpr int kEngineThreads = kWarpsPerCta * 32;
 constexpr int kGrab = 2;  // tiles taken per atomic
@@ -250,27 +253,46 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
     }
   }
 
-  // ---- 1. products into warp-private shared memory
-  for (int c0 = 0; c0 < nnz; c0 += 32 * kChunk) {
+  // ---- 1. products into warp-private shared memory.  The column indices and
+  // values of the next round are requested before the current round's
+  // gathers, so the DRAM stream and the L2 gathers overlap.
+  {
+    auto load_round = [&](int c0, int32_t* cc, double* vv) {
+#pragma unroll
+      for (int k = 0; k < kChunk; ++k) {
+        const int e = c0 + lane + 32 * k;
+        cc[k] = 0;
+        vv[k] = 0.0;
+        if (e < nnz) {
+          cc[k] = __ldcs(a.M.col + t.nzb + e);
+          if constexpr (PREC == HPR_PREC_FP64) vv[k] = __ldcs(a.M.val + t.nzb + e);
+          else vv[k] = (double)ldval32<PREC>(a.M, (int64_t)t.nzb + e);
+        }
+      }
+    };
     int32_t cols[kChunk];
     double vals[kChunk];
+    load_round(0, cols, vals);
+    for (int c0 = 0; c0 < nnz; c0 += 32 * kChunk) {
+      int32_t ncols[kChunk];
+      double nvals[kChunk];
+      if (HPR_ENGINE_PIPE && c0 + 32 * kChunk < nnz) load_round(c0 + 32 * kChunk, ncols, nvals);
 #pragma unroll
-    for (int k = 0; k < kChunk; ++k) {
-      int e = c0 + lane + 32 * k;
-      if (e < nnz) {
-        cols[k] = __ldcs(a.M.col + t.nzb + e);
-        if constexpr (PREC == HPR_PREC_FP64) vals[k] = __ldcs(a.M.val + t.nzb + e);
-        else vals[k] = (double)ldval32<PREC>(a.M, (int64_t)t.nzb + e);
+      for (int k = 0; k < kChunk; ++k) {
+        const int e = c0 + lane + 32 * k;
+        if (e < nnz) {
+          if constexpr (PREC == HPR_PREC_FP64)
+            ws.prod[e] = vals[k] * (kCoherent ? __ldcg(a.xin + cols[k]) : __ldg(a.xin + cols[k]));
+          else
+            ws.prod[e] =
+                (double)((float)vals[k] * (kCoherent ? __ldcg(a.xin32 + cols[k]) : __ldg(a.xin32 + cols[k])));
+        }
       }
-    }
+      if (!HPR_ENGINE_PIPE && c0 + 32 * kChunk < nnz) load_round(c0 + 32 * kChunk, ncols, nvals);
 #pragma unroll
-    for (int k = 0; k < kChunk; ++k) {
-      int e = c0 + lane + 32 * k;
-      if (e < nnz) {
-        if constexpr (PREC == HPR_PREC_FP64)
-          ws.prod[e] = vals[k] * (kCoherent ? __ldcg(a.xin + cols[k]) : __ldg(a.xin + cols[k]));
-        else
-          ws.prod[e] = (double)((float)vals[k] * (kCoherent ? __ldcg(a.xin32 + cols[k]) : __ldg(a.xin32 + cols[k])));
+      for (int k = 0; k < kChunk; ++k) {
+        cols[k] = ncols[k];
+        vals[k] = nvals[k];
       }
     }
   }
