@@ -285,6 +285,36 @@ def run_tts(args):
     print(json.dumps(line))
 
 
+def run_spmv_baseline(args):
+    """Library SpMV stand-in for the reference's GPU path: cuSPARSE CSR SpMV
+    (through torch.sparse CSR matvec) on the benchmark's A and A', timed
+    with CUDA events; the fused iteration does both products and every
+    epilogue in one pass each."""
+    import torch
+    from hprsocp_b200 import instances
+    model = instances.config1(1, scale=args.scale)
+    dev = torch.device("cuda")
+    out = {}
+    for name, M in (("A", model.A), ("AT", model.AT)):
+        T = torch.sparse_csr_tensor(torch.from_numpy(M.indptr.astype("int32")), torch.from_numpy(M.indices.astype("int32")),
+                                    torch.from_numpy(M.data), size=M.shape, device=dev)
+        x = torch.rand(M.shape[1], dtype=torch.float64, device=dev)
+        for _ in range(5):
+            y = T @ x
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(50):
+            y = T @ x
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 50
+        nbytes = M.nnz * 12 + (M.shape[0] + 1) * 4 + (M.shape[0] + M.shape[1]) * 8
+        out[name] = {"ms": ms, "GBs": nbytes / ms / 1e6, "nnz": int(M.nnz)}
+    print(json.dumps({"metric": "cuSPARSE CSR SpMV (torch.sparse matvec)", "config": {"workload": WORKLOAD},
+                      "spmv": out, "sum_ms": out["A"]["ms"] + out["AT"]["ms"]}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -294,7 +324,7 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the instance (testing only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", default="iterate", choices=["iterate", "serve", "tts"],
+    ap.add_argument("--mode", default="iterate", choices=["iterate", "serve", "tts", "spmv-baseline"],
                     help="serve: the small-SOCP serving stream; tts: time to 1e-6 per SpMV precision")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests in the stream")
     ap.add_argument("--slots", type=int, default=32, help="serve: concurrent solver slots")
@@ -307,6 +337,9 @@ def main():
         return
     if args.mode == "tts":
         run_tts(args)
+        return
+    if args.mode == "spmv-baseline":
+        run_spmv_baseline(args)
         return
 
     from hprsocp_b200 import instances
@@ -381,7 +414,10 @@ def main():
         iters = 3
         cpu_rate = cpu_iteration_rate(model, iters=iters, threads=0)
         cpu = {"value": cpu_rate, "unit": "iter/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"{iters} HPR iterations of the benchmark instance on the oracle (all host threads)"}
+               "sample": f"{iters} HPR iterations of the benchmark instance on the oracle (all host threads)",
+               "one_thread": {"value": cpu_iteration_rate(model, iters=1, threads=1), "unit": "iter/s",
+                              "cores": 1, "sample": "1 HPR iteration on one thread (the reference's CPU "
+                                                    "path is single-threaded)"}}
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "engine_config1_dram_bytes.txt")
     if os.path.exists(tfile):

@@ -656,6 +656,7 @@ int hpr_destroy(hpr_ctx* h) {
   if (c->h_state) cudaFreeHost(c->h_state);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ev_mid) cudaEventDestroy(c->ev_mid);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete h;
   return HPR_OK;
@@ -989,6 +990,15 @@ int hpr_set_precision(hpr_ctx* h, int mode) {
   if (mode != HPR_PREC_FP64 && mode != HPR_PREC_FP32 && mode != HPR_PREC_BF16)
     return set_err(c, HPR_E_BAD_INPUT, "unknown precision mode");
   return apply_precision(c, mode);
+}
+
+int hpr_set_schedule(hpr_ctx* h, int mode) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  if (mode != HPR_SCHEDULE_AUTO && mode != HPR_SCHEDULE_ENGINE && mode != HPR_SCHEDULE_FUSED)
+    return set_err(c, HPR_E_BAD_INPUT, "unknown schedule");
+  c->schedule = mode;
+  return HPR_OK;
 }
 
 int hpr_solve(hpr_ctx* h, const hpr_params* params, hpr_results* res) {

@@ -126,7 +126,8 @@ struct Ctx {
   size_t budget = 0, used = 0;
   std::unordered_map<void*, size_t> allocs;  // live device allocations and their sizes
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_mid = nullptr;
+  int schedule = HPR_SCHEDULE_AUTO;  // hpr_set_schedule
   bool uploaded = false, scaled = false;
   // problem
   int64_t m = 0, n = 0, m_lin = 0, n_box = 0;
@@ -215,7 +216,8 @@ int upload_plan(Ctx* c, Plan& p);
 PlanView view_of(const Plan& p, const int32_t* cone_start);
 int launch_iteration(Ctx* c, bool full);
 int run_iterations(Ctx* c, int64_t k, bool full_last);
-// true when run_iterations uses the single-CTA multi-iteration kernel
+// true when run_iterations may use the single-CTA multi-iteration kernel
+// (then no partial-iteration graph is captured)
 bool uses_fused_iterations(const Ctx* c);
 int launch_residuals(Ctx* c, bool include_bounds, hpr_residuals* out);
 int launch_residuals_noalloc(Ctx* c, bool include_bounds, hpr_residuals* out);

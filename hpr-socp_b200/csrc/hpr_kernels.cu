@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 
@@ -847,19 +848,12 @@ int launch_fused(Ctx* c, int64_t k, bool full_last) {
 
 }  // namespace
 
-bool uses_fused_iterations(const Ctx* c) { return fused_eligible(c); }
 
-int run_iterations(Ctx* c, int64_t k, bool full_last) {
-  if (k <= 0) return HPR_OK;
-  int64_t l0 = c->launches;
-  HPR_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-  if (fused_eligible(c)) {
-    HPR_TRY(launch_fused(c, k, full_last));
-    HPR_CUDA(c, cudaEventRecord(c->ev1, c->stream));
-    c->inner += k;
-    c->last_launches = c->launches - l0;
-    return HPR_OK;
-  }
+
+namespace {
+
+// Unfused path: engine launches (graph replays where captured).
+int run_engine_iterations(Ctx* c, int64_t k, bool full_last) {
   int64_t partial = full_last ? k - 1 : k;
   int64_t done = 0;
   // replay the captured partial-iteration graph where it fits
@@ -872,6 +866,76 @@ int run_iterations(Ctx* c, int64_t k, bool full_last) {
   }
   for (; done < partial; ++done) HPR_TRY(launch_iteration(c, false));
   if (full_last) HPR_TRY(launch_iteration(c, true));
+  return HPR_OK;
+}
+
+// Schedule autotuner.  Problems small enough for the single-CTA fused kernel
+// can also run on the multi-CTA engine; which is faster depends on how many
+// tiles a side has.  The first batch of at least 16 iterations of a size
+// class runs half on each path (the iterates are identical either way),
+// times both with events and records the faster per iteration for the
+// class; later batches of the class in this process use the recorded choice.
+std::mutex g_tune_mu;
+std::map<int, int> g_tune;  // class -> HPR_SCHEDULE_ENGINE / _FUSED
+
+int tune_class(const Ctx* c) {
+  int64_t t = std::max<int64_t>((int64_t)c->planX.tasks.size(), (int64_t)c->planY.tasks.size());
+  if (c->has_q) t = std::max<int64_t>(t, (int64_t)c->planQ.tasks.size());
+  int b = 0;
+  while ((1LL << b) < t) ++b;
+  return (c->has_q ? 100 : 0) + b;
+}
+
+int tune_lookup(const Ctx* c) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(tune_class(c));
+  return it == g_tune.end() ? HPR_SCHEDULE_AUTO : it->second;
+}
+
+int tune_trial(Ctx* c, int64_t k, bool full_last) {
+  if (!c->ev_mid) HPR_CUDA(c, cudaEventCreate(&c->ev_mid));
+  const int64_t k1 = k / 2;
+  HPR_TRY(launch_fused(c, k1, false));
+  HPR_CUDA(c, cudaEventRecord(c->ev_mid, c->stream));
+  HPR_TRY(run_engine_iterations(c, k - k1, full_last));
+  HPR_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+  HPR_CUDA(c, cudaEventSynchronize(c->ev1));
+  float tf = 0.f, te = 0.f;
+  HPR_CUDA(c, cudaEventElapsedTime(&tf, c->ev0, c->ev_mid));
+  HPR_CUDA(c, cudaEventElapsedTime(&te, c->ev_mid, c->ev1));
+  const int pick = (tf / (double)k1 <= te / (double)(k - k1)) ? HPR_SCHEDULE_FUSED : HPR_SCHEDULE_ENGINE;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune.emplace(tune_class(c), pick);
+  return HPR_OK;
+}
+
+}  // namespace
+
+bool uses_fused_iterations(const Ctx* c) {
+  if (!fused_eligible(c)) return false;
+  const int mode = c->schedule != HPR_SCHEDULE_AUTO ? c->schedule : tune_lookup(c);
+  return mode != HPR_SCHEDULE_ENGINE;
+}
+
+int run_iterations(Ctx* c, int64_t k, bool full_last) {
+  if (k <= 0) return HPR_OK;
+  int64_t l0 = c->launches;
+  HPR_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+  int mode = HPR_SCHEDULE_ENGINE;
+  if (fused_eligible(c)) {
+    mode = c->schedule != HPR_SCHEDULE_AUTO ? c->schedule : tune_lookup(c);
+    if (mode == HPR_SCHEDULE_AUTO) {
+      if (k >= 16) {
+        HPR_TRY(tune_trial(c, k, full_last));
+        c->inner += k;
+        c->last_launches = c->launches - l0;
+        return HPR_OK;
+      }
+      mode = HPR_SCHEDULE_FUSED;
+    }
+  }
+  if (mode == HPR_SCHEDULE_FUSED) HPR_TRY(launch_fused(c, k, full_last));
+  else HPR_TRY(run_engine_iterations(c, k, full_last));
   HPR_CUDA(c, cudaEventRecord(c->ev1, c->stream));
   c->inner += k;
   c->last_launches = c->launches - l0;

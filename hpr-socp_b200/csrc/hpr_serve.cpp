@@ -22,6 +22,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <set>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -134,6 +135,7 @@ struct hpr_server {
   std::condition_variable cv_work, cv_done;
   std::deque<Request> queue;
   std::map<int64_t, Finished> done;
+  std::set<int64_t> live;  // submitted and not yet consumed by a poll
   std::vector<std::thread> workers;
   int64_t next_ticket = 1;
   int64_t running = 0;
@@ -249,6 +251,7 @@ int hpr_serve_submit(hpr_server* s, const hpr_problem* prob, const hpr_params* p
     std::lock_guard<std::mutex> lk(s->mu);
     r.ticket = s->next_ticket++;
     *ticket = r.ticket;
+    s->live.insert(r.ticket);
     s->queue.push_back(std::move(r));
   }
   s->cv_work.notify_all();
@@ -258,15 +261,23 @@ int hpr_serve_submit(hpr_server* s, const hpr_problem* prob, const hpr_params* p
 int hpr_serve_poll(hpr_server* s, int64_t ticket, int wait_ms, hpr_results* res, double* latency_s) {
   if (!s || ticket <= 0) return HPR_E_BAD_INPUT;
   std::unique_lock<std::mutex> lk(s->mu);
-  if (ticket >= s->next_ticket) return HPR_E_BAD_INPUT;
-  auto ready = [&] { return s->done.count(ticket) > 0; };
+  if (!s->live.count(ticket)) {
+    s->err = "unknown or already consumed ticket " + std::to_string(ticket);
+    return HPR_E_BAD_INPUT;
+  }
+  auto ready = [&] { return s->done.count(ticket) > 0 || s->stop; };
   if (wait_ms < 0) {
     s->cv_done.wait(lk, ready);
   } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), ready)) {
     return HPR_E_TIMEOUT;
   }
+  if (!s->done.count(ticket)) {
+    s->err = "the server was stopped before this request finished";
+    return HPR_E_STATE;
+  }
   Finished f = std::move(s->done[ticket]);
   s->done.erase(ticket);
+  s->live.erase(ticket);
   lk.unlock();
   if (latency_s) *latency_s = f.latency;
   if (f.rc != HPR_OK) {
@@ -307,6 +318,7 @@ int hpr_serve_destroy(hpr_server* s) {
     s->stop = true;
   }
   s->cv_work.notify_all();
+  s->cv_done.notify_all();
   for (std::thread& t : s->workers) t.join();
   delete s;
   return HPR_OK;

@@ -41,6 +41,8 @@ SOC_SCALE_STRATEGIES = {
 
 HPR_PREC = {"fp64": 0, "fp32": 1, "bf16": 2}
 
+HPR_SCHEDULE = {"auto": 0, "engine": 1, "fused": 2}
+
 HPR_STATUS = {0: "OPTIMAL", 1: "MAX_ITER", 2: "TIME_LIMIT"}
 
 VEC = {
@@ -136,6 +138,7 @@ PROTOTYPES = {
     "hpr_set_vector": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_size_t]),
     "hpr_get_solution": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     "hpr_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "hpr_set_schedule": (C.c_int, [C.c_void_p, C.c_int]),
     "hpr_solve": (C.c_int, [C.c_void_p, C.POINTER(hpr_params), C.POINTER(hpr_results)]),
     "hpr_optimize": (C.c_int, [C.POINTER(hpr_problem), C.POINTER(hpr_params),
                                C.POINTER(hpr_results)]),

@@ -41,6 +41,8 @@ class Server:
 
     def poll(self, ticket: int, wait_ms: int = -1):
         """(HPRSOCP_results, latency_s), or None if not finished within wait_ms."""
+        if ticket not in self._shapes:
+            raise _abi.HPRError(_abi.HPR_E_BAD_INPUT, f"unknown or already consumed ticket {ticket}")
         m, n = self._shapes[ticket]
         x, y, z, w = np.zeros(n), np.zeros(m), np.zeros(n), np.zeros(n)
         r = _abi.hpr_results()

@@ -262,6 +262,10 @@ class Context:
         self._check(self.lib.hpr_get_solution(self.h, _abi.dptr(x), _abi.dptr(y), _abi.dptr(z), _abi.dptr(w)))
         return x, y, z, w
 
+    def set_schedule(self, mode: str):
+        """'auto' (timed choice per size class), 'engine' or 'fused'."""
+        self._check(self.lib.hpr_set_schedule(self.h, _abi.HPR_SCHEDULE[mode]))
+
     def set_precision(self, mode: str):
         self._check(self.lib.hpr_set_precision(self.h, _abi.HPR_PREC[mode]))
 

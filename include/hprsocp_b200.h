@@ -341,6 +341,18 @@ int hpr_set_vector(hpr_ctx* ctx, int which, const double* host, size_t len);
  * pointers may be NULL.                                                     */
 int hpr_get_solution(hpr_ctx* ctx, double* x, double* y, double* z, double* w);
 
+/* Iteration schedule (no counterpart in the reference, whose iteration is
+ * always a sequence of separate kernels).  Problems whose matrix sides have
+ * at most 32 warp tiles can run either on the multi-CTA engine (2 launches
+ * per iteration, 4 with Q) or on one CTA that runs a whole batch of
+ * iterations in a single launch.  AUTO (the default) times both on the
+ * first batch of a size class in the process and keeps the faster; ENGINE
+ * and FUSED force one.  The iterates are identical on every schedule.      */
+#define HPR_SCHEDULE_AUTO 0
+#define HPR_SCHEDULE_ENGINE 1
+#define HPR_SCHEDULE_FUSED 2
+int hpr_set_schedule(hpr_ctx* ctx, int mode);
+
 /* Precision of the A / A' stream (HPR_PREC_*); re-packs the scaled values.  */
 int hpr_set_precision(hpr_ctx* ctx, int mode);
 
@@ -389,8 +401,9 @@ int hpr_serve_submit(hpr_server* srv, const hpr_problem* prob,
 /* Wait up to wait_ms (< 0: forever) for a ticket.  HPR_OK: `res` holds the
  * result (x/y/z/w copied into the caller's buffers when non-NULL) and
  * latency_s the time from submit to completion; the ticket is consumed.
- * HPR_E_TIMEOUT: not finished yet.  Any other code: the solve's error
- * (message in hpr_serve_last_error).                                        */
+ * HPR_E_TIMEOUT: not finished yet.  HPR_E_BAD_INPUT: unknown or already
+ * consumed ticket.  HPR_E_STATE: the server was stopped first.  Any other
+ * code: the solve's error (message in hpr_serve_last_error).                */
 int hpr_serve_poll(hpr_server* srv, int64_t ticket, int wait_ms,
                    hpr_results* res, double* latency_s);
 

@@ -157,3 +157,24 @@ def test_solve_parity_small(models, name):
     assert ro.status == rg.status == "OPTIMAL"
     assert abs(rg.primal_obj - ro.primal_obj) <= 1e-6 * max(1.0, abs(ro.primal_obj))
     assert abs(rg.iter - ro.iter) <= max(10, ro.iter // 20), (rg.iter, ro.iter)
+
+
+@pytest.mark.parametrize("name", ["small_noq", "small_q"])
+def test_schedules_give_identical_iterates(models, name):
+    """The single-CTA multi-iteration kernel and the multi-CTA engine run
+    the same per-row arithmetic: 300 iterations (two batches) agree bit for
+    bit."""
+    from hprsocp_b200 import Context
+    res = {}
+    for mode in ("engine", "fused", "auto"):
+        with Context(models[name]) as g:
+            g.set_schedule(mode)
+            info = g.scale(HPRSOCP_parameters(verbose=False))
+            g.set_sigma_lambda(info["norm_b"] / info["norm_c"], 1.05 * g.power_A(), 0.0)
+            g.set_inner(0)
+            g.iterate(150, True)
+            g.iterate(150, True)
+            res[mode] = [g.get(v) for v in VECS]
+    for mode in ("fused", "auto"):
+        for a, b in zip(res[mode], res["engine"]):
+            assert np.array_equal(a, b), mode

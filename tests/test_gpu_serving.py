@@ -59,3 +59,17 @@ def test_admission_by_hbm_budget(stream):
         with pytest.raises(_abi.HPRError) as e:
             srv.submit(big, _params(1e-4))
         assert e.value.code == _abi.HPR_E_BUDGET
+
+
+def test_a_ticket_is_consumed_by_its_poll(stream):
+    with Server(slots=2) as srv:
+        t = srv.submit(stream[0][0], _params(1e-4))
+        r, _ = srv.poll(t)
+        assert r.status == "OPTIMAL"
+        with pytest.raises(_abi.HPRError) as e:
+            srv.poll(t)
+        assert e.value.code == _abi.HPR_E_BAD_INPUT
+        # the C entry point refuses it as well
+        import ctypes as C
+        lat = C.c_double()
+        assert srv.lib.hpr_serve_poll(srv.h, t, 0, None, C.byref(lat)) == _abi.HPR_E_BAD_INPUT
