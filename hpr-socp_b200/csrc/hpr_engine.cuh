@@ -162,6 +162,9 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #ifndef HPR_ENGINE_CHUNK
 #define HPR_ENGINE_CHUNK 2
 #endif
+#ifndef HPR_ENGINE_EARLYGRAB
+#define HPR_ENGINE_EARLYGRAB 0
+#endif
 #ifndef HPR_ENGINE_PIPE
 #define HPR_ENGINE_PIPE 1  // next round's col/val requested before this round's gathers
 #endif
@@ -229,8 +232,12 @@ __device__ __forceinline__ bool arrive_big(const EngineArgs& a, int slot) {
 // kCoherent: the gathered vector may have been written earlier in the same
 // launch (the fused multi-iteration kernel), so it is read through L2
 // instead of the read-only path.
-template <class Epi, int PREC, bool kCoherent = false>
+// CH: nonzeros per lane per gather round (the multi-CTA engine uses kChunk;
+// the single-CTA kernels, with few warps in flight, load a whole tile per
+// round).
+template <class Epi, int PREC, bool kCoherent = false, int CH = kChunk>
 __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSmem& ws) {
+  constexpr int kChunk = CH;
   const int lane = threadIdx.x & 31;
   const Task t = a.pv.tasks[tix];
   const int nrows = t.re - t.rb;
@@ -449,12 +456,17 @@ __global__ void __launch_bounds__(kEngineThreads, HPR_ENGINE_MINB) engine_kernel
   const int ntasks = a.pv.ntasks;
   epi.setup(a.st);
   WarpSmem& ws = s_ws[wid];
-  for (;;) {
-    int base = 0;
-    if (lane == 0) base = atomicAdd(a.pv.task_ctr, kGrab);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= ntasks) break;
+  int base = 0;
+  if (lane == 0) base = atomicAdd(a.pv.task_ctr, kGrab);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  while (base < ntasks) {
+    // with HPR_ENGINE_EARLYGRAB the next grab is requested before this one is
+    // processed, so its atomic latency is hidden behind the tiles
+    int next = 0;
+    if (HPR_ENGINE_EARLYGRAB && lane == 0) next = atomicAdd(a.pv.task_ctr, kGrab);
     for (int q = 0; q < kGrab && base + q < ntasks; ++q) process_warp_tile<Epi, PREC>(a, epi, base + q, ws);
+    if (!HPR_ENGINE_EARLYGRAB && lane == 0) next = atomicAdd(a.pv.task_ctr, kGrab);
+    base = __shfl_sync(0xffffffffu, next, 0);
   }
   // ---- last warp: reset the tile counter, advance the Halpern counter
   if (lane == 0) {

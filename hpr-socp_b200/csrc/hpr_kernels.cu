@@ -741,6 +741,10 @@ int launch_iteration(Ctx* c, bool full) {
 #define HPR_FUSED_MAX_TILES (4 * kWarpsPerCta)
 #endif
 constexpr int kFusedMaxTiles = HPR_FUSED_MAX_TILES;
+#ifndef HPR_FUSED_CHUNK
+#define HPR_FUSED_CHUNK 8
+#endif
+constexpr int kFusedChunk = HPR_FUSED_CHUNK;  // 256 nonzeros of a tile per round
 
 namespace {
 
@@ -756,7 +760,8 @@ __device__ __forceinline__ void fused_stage(const FStage<E>& s, bool last, WarpS
   if (!s.on) return;
   E e = last ? s.full : s.part;
   e.setup(s.a.st);
-  for (int t = threadIdx.x >> 5; t < s.a.pv.ntasks; t += kWarpsPerCta) process_warp_tile<E, PREC, true>(s.a, e, t, ws);
+  for (int t = threadIdx.x >> 5; t < s.a.pv.ntasks; t += kWarpsPerCta)
+    process_warp_tile<E, PREC, true, kFusedChunk>(s.a, e, t, ws);
   __syncthreads();
 }
 
