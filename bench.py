@@ -315,6 +315,24 @@ def run_spmv_baseline(args):
                       "spmv": out, "sum_ms": out["A"]["ms"] + out["AT"]["ms"]}))
 
 
+def run_gather_ceiling(args):
+    """The device's random-gather rate for a 25M-nonzero SpMV pattern (the
+    bound that a random-column SpMV meets before DRAM bandwidth), against
+    the gathers the benchmark iteration achieves."""
+    import ctypes as C
+    from hprsocp_b200 import _abi
+    lib = _abi.load_library()
+    res = {}
+    for nx in (1_500_000, 2_000_000):
+        ms, rate = C.c_double(), C.c_double()
+        rc = lib.hpr_probe_gather(0, 24_972_397, nx, C.byref(ms), C.byref(rate))
+        if rc != 0:
+            raise RuntimeError(f"hpr_probe_gather failed: {rc}")
+        res[str(nx)] = {"ms": ms.value, "gathers_per_s": rate.value}
+    print(json.dumps({"metric": "random gathers/s", "n": 24_972_397, "vector_lengths": res,
+                      "floor_ms_per_iteration": sum(r["ms"] for r in res.values())}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -324,7 +342,7 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the instance (testing only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", default="iterate", choices=["iterate", "serve", "tts", "spmv-baseline"],
+    ap.add_argument("--mode", default="iterate", choices=["iterate", "serve", "tts", "spmv-baseline", "gather-ceiling"],
                     help="serve: the small-SOCP serving stream; tts: time to 1e-6 per SpMV precision")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests in the stream")
     ap.add_argument("--slots", type=int, default=32, help="serve: concurrent solver slots")
@@ -340,6 +358,9 @@ def main():
         return
     if args.mode == "spmv-baseline":
         run_spmv_baseline(args)
+        return
+    if args.mode == "gather-ceiling":
+        run_gather_ceiling(args)
         return
 
     from hprsocp_b200 import instances

@@ -170,7 +170,7 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #endif
 constexpr int kWarpsPerCta = HPR_ENGINE_WARPS;
 constexpr int kEngineThreads = kWarpsPerCta * 32;
-constexpr int kGrab = 2;  // tiles taken per atomic
+constexpr int kGrab = 1;  // tiles taken per atomic
 constexpr int kChunk = HPR_ENGINE_CHUNK;  // elements per lane per gather round
 constexpr bool kTwoRows = kRowCap > 32;   // a lane owns rows lane and lane + 32
 

@@ -144,6 +144,7 @@ PROTOTYPES = {
                                C.POINTER(hpr_results)]),
     "hpr_last_iterate_ms": (C.c_int, [C.c_void_p, _dp, _lp]),
     "hpr_iteration_bytes": (C.c_int, [C.c_void_p, _dp]),
+    "hpr_probe_gather": (C.c_int, [C.c_int, C.c_int64, C.c_int64, _dp, _dp]),
     "hpr_serve_create": (C.c_int, [C.c_int, C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]),
     "hpr_serve_submit": (C.c_int, [C.c_void_p, C.POINTER(hpr_problem), C.POINTER(hpr_params), _lp]),
     "hpr_serve_poll": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.POINTER(hpr_results), _dp]),

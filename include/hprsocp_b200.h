@@ -379,6 +379,14 @@ int hpr_last_iterate_ms(hpr_ctx* ctx, double* ms_total, int64_t* launches);
  * roofline numerator used by the benchmark).                               */
 int hpr_iteration_bytes(hpr_ctx* ctx, double* bytes_per_iter);
 
+/* Diagnostic (no counterpart in the reference): the device's rate for the
+ * access pattern of a random-column SpMV, n streamed (column, value) pairs
+ * each gathering one double from a vector of nx entries, with no solver
+ * work around it.  Returns the milliseconds of one pass and the gathers per
+ * second.  Allocates its own buffers (about 12n + 8nx bytes).             */
+int hpr_probe_gather(int device, int64_t n, int64_t nx, double* ms,
+                     double* gathers_per_s);
+
 /* ------------------------------------------------------------------------ */
 /* Serving: continuous batching of many small problems on one device.       */
 /* No single reference counterpart: it replaces calling optimize() once per */
