@@ -162,6 +162,9 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #ifndef HPR_ENGINE_CHUNK
 #define HPR_ENGINE_CHUNK 2
 #endif
+#ifndef HPR_ENGINE_PREFETCH
+#define HPR_ENGINE_PREFETCH 1  // epilogue inputs loaded before the gather rounds
+#endif
 #ifndef HPR_ENGINE_EARLYGRAB
 #define HPR_ENGINE_EARLYGRAB 0
 #endif
@@ -251,12 +254,12 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
     if (lane < nrows) {
       r0b = __ldg(a.M.rowptr + t.rb + lane) - t.nzb;
       r0e = __ldg(a.M.rowptr + t.rb + lane + 1) - t.nzb;
-      load_vals<Epi>(v0, epi, cone, t.rb + lane);
+      if (HPR_ENGINE_PREFETCH) load_vals<Epi>(v0, epi, cone, t.rb + lane);
     }
     if (kTwoRows && lane + 32 < nrows) {
       r1b = __ldg(a.M.rowptr + t.rb + lane + 32) - t.nzb;
       r1e = __ldg(a.M.rowptr + t.rb + lane + 33) - t.nzb;
-      load_vals<Epi>(v1, epi, cone, t.rb + lane + 32);
+      if (HPR_ENGINE_PREFETCH) load_vals<Epi>(v1, epi, cone, t.rb + lane + 32);
     }
   }
 
@@ -350,6 +353,12 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
     return;
   }
 
+  // without the prefetch, the epilogue inputs are requested here, so they
+  // are not live in registers during the gather rounds
+  if (!HPR_ENGINE_PREFETCH) {
+    if (lane < nrows) load_vals<Epi>(v0, epi, cone, t.rb + lane);
+    if (kTwoRows && lane + 32 < nrows) load_vals<Epi>(v1, epi, cone, t.rb + lane + 32);
+  }
   // ---- 2. row sums
   bool long0 = false, long1 = false;
   if (lane < nrows) {
