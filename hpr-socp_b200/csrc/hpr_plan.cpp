@@ -17,6 +17,10 @@
 
 #include "hpr_internal.h"
 
+#ifndef HPR_PLAN_LPT
+#define HPR_PLAN_LPT 0
+#endif
+
 namespace hpr {
 
 namespace {
@@ -167,6 +171,11 @@ void build_plan(const std::vector<int32_t>& rp, int64_t nrows,
     }
   }
   flush();
+#if HPR_PLAN_LPT
+  // longest first: the tiles that end a launch are the lightest ones
+  std::stable_sort(rows.begin(), rows.end(),
+                   [](const Task& x, const Task& y) { return (x.nze - x.nzb) > (y.nze - y.nzb); });
+#endif
   plan.tasks = multi;
   plan.tasks.insert(plan.tasks.end(), rows.begin(), rows.end());
   // flag tiles holding rows that need the warp-reduction phase
