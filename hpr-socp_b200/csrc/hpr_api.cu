@@ -770,13 +770,15 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
     HPR_TRY(put_vec(c, &c->soc_rhs_full, full.data(), m));
   }
   // workspace (allocate_workspace, algorithm.jl:1443-1588)
-  double** nvecs[] = {&c->row_norm, &c->col_norm, &c->diag_Q, &c->fact1, &c->fact2, &c->fact,  &c->fact_M,
+  // length-n vectors (the variable side)
+  double** nvecs[] = {&c->col_norm, &c->diag_Q, &c->fact1, &c->fact2, &c->fact,  &c->fact_M,
                       &c->x,        &c->x_hat,    &c->x_bar,  &c->last_x, &c->z_bar, &c->dx,   &c->w,
                       &c->w_bar,    &c->last_w,   &c->dw,     &c->Qw,     &c->dQw,   &c->Qx,   &c->tempv,
                       &c->ATy,      &c->ATy_bar,  &c->last_ATy, &c->ATdy, &c->QATdy, &c->Rd,   &c->vtmp_n,
                       &c->ptq};
   for (double** v2 : nvecs) HPR_TRY(zero_vec(c, v2, n));
-  double** mvecs[] = {&c->y, &c->y_bar, &c->last_y, &c->s, &c->dy, &c->Rp, &c->Ax, &c->vtmp_m};
+  // length-m vectors (the constraint side)
+  double** mvecs[] = {&c->row_norm, &c->y, &c->y_bar, &c->last_y, &c->s, &c->dy, &c->Rp, &c->Ax, &c->vtmp_m};
   for (double** v2 : mvecs) HPR_TRY(zero_vec(c, v2, m));
   HPR_TRY(zero_vec(c, &c->pz, std::max(m, n)));
   HPR_TRY(zero_vec(c, &c->pq, std::max(m, n)));

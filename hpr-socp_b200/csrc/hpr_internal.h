@@ -191,12 +191,16 @@ struct Ctx {
 
 // error helpers
 int set_err(Ctx* c, int code, const std::string& msg);
+// (a failed call's error is also taken off the runtime's last-error slot, so
+// a later cudaGetLastError() check does not report it again)
 #define HPR_CUDA(ctx, call)                                                 \
   do {                                                                      \
     cudaError_t e_ = (call);                                                \
-    if (e_ != cudaSuccess)                                                  \
+    if (e_ != cudaSuccess) {                                                \
+      (void)cudaGetLastError();                                             \
       return ::hpr::set_err((ctx), HPR_E_CUDA,                              \
                             std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    }                                                                       \
   } while (0)
 #define HPR_TRY(...)                 \
   do {                               \

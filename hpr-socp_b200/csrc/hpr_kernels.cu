@@ -310,6 +310,47 @@ struct EpiDot {
   __device__ void cone_apply(int64_t, double, double, double, bool, const In&, Red&) {}
 };
 
+// Power-iteration half-steps (two SpMVs per iteration instead of two SpMVs
+// and seven vector kernels):
+// out = (M v) / |z|, with |z|^2 read from the device (the normalisation of
+// the iterate folded into the first product)
+struct EpiScale {
+  static constexpr bool kCones = false;
+  static constexpr int kNRed = 0;
+  static constexpr unsigned kMaxMask = 0;
+  static constexpr int kSlots = 0;
+  using In = Vals<kSlots>;
+  const double* lin_src[1];
+  const double* cone_src[1];
+  double* out;
+  const double* nz2;  // |z|^2
+  double inv;
+  __device__ void setup(const DevState*) { inv = 1.0 / sqrt(*nz2); }
+  __device__ void linear(int64_t i, double v, const In&, Red&) { out[i] = v * inv; }
+  __device__ double cone_raw(int64_t, double v, const In&, Red&) { return v; }
+  __device__ void cone_apply(int64_t, double, double, double, bool, const In&, Red&) {}
+};
+
+// out = M v with lanes 0: |out|^2, 1: <zold, out>.   slots: 0 zold
+struct EpiPow {
+  static constexpr bool kCones = false;
+  static constexpr int kNRed = 2;
+  static constexpr unsigned kMaxMask = 0;
+  static constexpr int kSlots = 1;
+  using In = Vals<kSlots>;
+  const double* lin_src[kSlots];
+  const double* cone_src[kSlots];
+  double* out;
+  __device__ void setup(const DevState*) {}
+  __device__ void linear(int64_t i, double v, const In& in, Red& r) {
+    out[i] = v;
+    r.v[0] = r.v[0] + v * v;
+    r.v[1] = r.v[1] + in(0, i) * v;
+  }
+  __device__ double cone_raw(int64_t, double v, const In&, Red&) { return v; }
+  __device__ void cone_apply(int64_t, double, double, double, bool, const In&, Red&) {}
+};
+
 // Dual residual in original coordinates: compute_Rd_kernel! /
 // compute_Rd_noQ_kernel! (kernels.jl:6467-6512) with the objective dots of
 // compute_residuals! (algorithm.jl:113-160).
@@ -1356,6 +1397,47 @@ int power_generic(Ctx* c, int64_t len, bool isA, int maxit, double tol, double* 
 }
 }  // namespace
 
+// The power iteration on lambda_max(AA') for large problems.  Per iteration
+// q = z/|z| is folded into the first product (tq = A'z / |z|), and
+// lambda = <q, znew> = <z, znew>/|z| and |znew - lambda q|^2 =
+// |znew|^2 - lambda^2 come from reductions in the second product's
+// epilogue, so an iteration is two engine launches, one reduction finish
+// and one read-back.  Same steps and stopping rule as power_generic.
+int power_two_pass_A(Ctx* c, int maxit, double tol, double* lam) {
+  const int64_t m = c->m;
+  std::vector<double> hz(m);
+  power_start_vector(hz, 1);
+  double* zb[2] = {c->pz, c->pq};
+  HPR_CUDA(c, cudaMemcpyAsync(zb[0], hz.data(), m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  double* out = c->d_red_out;
+  const double* zz = zb[0];
+  HPR_TRY(vec_reduce<1, 0>(c, m, DotF{zz, zz}, 30));  // |z0|^2 into out[30]
+  HPR_TRY(fetch_red(c, 31));
+  double nz2 = c->h_red_out[30];
+  double lambda = 1.0;
+  int cur = 0;
+  for (int it = 0; it < maxit; ++it) {
+    EpiScale es{};
+    es.out = c->ptq;
+    es.nz2 = out + 30;
+    HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, zb[cur], nullptr, es, false, false, 0));
+    EpiPow ep{};
+    ep.lin_src[0] = ep.cone_src[0] = zb[cur];
+    ep.out = zb[cur ^ 1];
+    HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->ptq, nullptr, ep, false, true, 30));
+    HPR_TRY(fetch_red(c, 32));
+    const double nn2 = c->h_red_out[30], dot = c->h_red_out[31];
+    lambda = dot / std::sqrt(nz2);
+    const double r2 = std::max(nn2 - lambda * lambda, 0.0);
+    const double err = std::sqrt(r2) / (std::sqrt(nn2) + lambda);
+    nz2 = nn2;
+    cur ^= 1;
+    if (err < tol) break;
+  }
+  *lam = lambda;
+  return HPR_OK;
+}
+
 int launch_power_A(Ctx* c, int maxit, double tol, double* lam) {
   if (c->m == 0) {
     *lam = 0.0;
@@ -1363,7 +1445,7 @@ int launch_power_A(Ctx* c, int maxit, double tol, double* lam) {
   }
   auto small = [](const Plan& p) { return (int64_t)p.tasks.size() <= kFusedMaxTiles; };
   if (small(c->planX) && small(c->planY) && kEngineSmem <= 48 * 1024) return power_fused_A(c, maxit, tol, lam);
-  return power_generic(c, c->m, true, maxit, tol, lam);
+  return power_two_pass_A(c, maxit, tol, lam);
 }
 
 int launch_power_Q(Ctx* c, int maxit, double tol, double* lam) {

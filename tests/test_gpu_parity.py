@@ -25,7 +25,10 @@ def models():
     return {"config0": instances.config0(0), "stress": stress_model(5),
             "config1_small": instances.config1(11, scale=0.004),
             "small_noq": instances.small_socp(21, n=300, diag_q=False),
-            "small_q": instances.small_socp(22, n=300, diag_q=True)}
+            "small_q": instances.small_socp(22, n=300, diag_q=True),
+            # Q = D + F'F applied as an operator (no scaling, as the reference
+            # does for operator Q)
+            "config2_small": instances.config2(2, scale=0.01)}
 
 
 def _pair(model):
@@ -38,14 +41,17 @@ def _setup(o, g, params=None):
     so = o.scale(params)
     sg = g.scale(params)
     lam = o.power_A() * 1.05
+    # operator Q (D + F'F): lambda_max(Q) by the power iteration, injected
+    # identically on both sides; CSR Q keeps 0 (its factors use diag(Q))
+    lamq = o.power_Q() * 1.05 if getattr(o.model, "F", None) is not None else 0.0
     sigma = so["norm_b"] / so["norm_c"] if so["norm_c"] > 1e-16 else 1.0
     for c in (o, g):
-        c.set_sigma_lambda(sigma, lam, 0.0)
+        c.set_sigma_lambda(sigma, lam, lamq)
         c.set_inner(0)
     return so, sg
 
 
-@pytest.mark.parametrize("name", ["config0", "stress", "config1_small"])
+@pytest.mark.parametrize("name", ["config0", "stress", "config1_small", "config2_small"])
 def test_scaling_parity(models, name):
     o, g = _pair(models[name])
     so = o.scale(HPRSOCP_parameters(verbose=False))
@@ -62,7 +68,7 @@ def test_scaling_parity(models, name):
         assert rel_err(a[fin], b[fin]) <= SCALE_TOL, v
 
 
-@pytest.mark.parametrize("name", ["config0", "stress", "config1_small", "small_noq", "small_q"])
+@pytest.mark.parametrize("name", ["config0", "stress", "config1_small", "small_noq", "small_q", "config2_small"])
 @pytest.mark.parametrize("K", [1, 150, 1000])
 def test_iterate_parity(models, name, K):
     o, g = _pair(models[name])
@@ -148,7 +154,7 @@ def test_solve_is_deterministic(models):
     assert np.array_equal(r1.x, r2.x) and np.array_equal(r1.y, r2.y)
 
 
-@pytest.mark.parametrize("name", ["small_noq", "small_q"])
+@pytest.mark.parametrize("name", ["small_noq", "small_q", "config2_small"])
 def test_solve_parity_small(models, name):
     p = HPRSOCP_parameters(verbose=False, stoptol=1e-6, max_iter=100000)
     o, g = _pair(models[name])
