@@ -62,3 +62,20 @@ def stress_model(seed=5, with_long_rows=True):
     A1 = instances._random_rows(rng, m1, n, len1)
     A2 = instances._random_rows(rng, m2, n, len2)
     return instances._assemble(rng, A1, A2, n_box, var_dims, con_dims)
+
+
+def tall_model(seed=3):
+    """More constraint rows than variables (m > n), with boxed and cone
+    variables and linear and cone rows: every length-m buffer is exercised
+    beyond n."""
+    import scipy.sparse as sp
+    from hprsocp_b200 import instances
+    rng = np.random.default_rng(seed)
+    n, n_box = 300, 200
+    var_dims = [5] * 20
+    con_dims = [4] * 50 + [40] * 2
+    m1 = 420
+    A1 = sp.random(m1, n, density=0.03, random_state=rng, data_rvs=rng.standard_normal, format="csr")
+    A2 = sp.random(int(np.sum(con_dims)), n, density=0.03, random_state=rng, data_rvs=rng.standard_normal,
+                   format="csr")
+    return instances._assemble(rng, A1, A2, n_box, var_dims, con_dims)

@@ -8,7 +8,7 @@ the objective within 1e-6 relative of the oracle's.
 import numpy as np
 import pytest
 
-from helpers import rel_err, stress_model
+from helpers import rel_err, stress_model, tall_model
 from hprsocp_b200 import HPRSOCP_parameters, instances
 from oracle_ctx import OracleContext
 
@@ -28,7 +28,8 @@ def models():
             "small_q": instances.small_socp(22, n=300, diag_q=True),
             # Q = D + F'F applied as an operator (no scaling, as the reference
             # does for operator Q)
-            "config2_small": instances.config2(2, scale=0.01)}
+            "config2_small": instances.config2(2, scale=0.01),
+            "tall": tall_model(3)}
 
 
 def _pair(model):
@@ -51,7 +52,7 @@ def _setup(o, g, params=None):
     return so, sg
 
 
-@pytest.mark.parametrize("name", ["config0", "stress", "config1_small", "config2_small"])
+@pytest.mark.parametrize("name", ["config0", "stress", "config1_small", "config2_small", "tall"])
 def test_scaling_parity(models, name):
     o, g = _pair(models[name])
     so = o.scale(HPRSOCP_parameters(verbose=False))
@@ -68,7 +69,8 @@ def test_scaling_parity(models, name):
         assert rel_err(a[fin], b[fin]) <= SCALE_TOL, v
 
 
-@pytest.mark.parametrize("name", ["config0", "stress", "config1_small", "small_noq", "small_q", "config2_small"])
+@pytest.mark.parametrize("name", ["config0", "stress", "config1_small", "small_noq", "small_q", "config2_small",
+                                  "tall"])
 @pytest.mark.parametrize("K", [1, 150, 1000])
 def test_iterate_parity(models, name, K):
     o, g = _pair(models[name])
@@ -96,7 +98,7 @@ def test_single_iteration_is_bit_exact_on_serial_rows(models):
         assert np.array_equal(g.get(v), o.get(v)), v
 
 
-@pytest.mark.parametrize("name", ["config0", "stress"])
+@pytest.mark.parametrize("name", ["config0", "stress", "tall", "config2_small"])
 def test_residual_mnorm_sigma_parity(models, name):
     o, g = _pair(models[name])
     _setup(o, g)
@@ -154,7 +156,7 @@ def test_solve_is_deterministic(models):
     assert np.array_equal(r1.x, r2.x) and np.array_equal(r1.y, r2.y)
 
 
-@pytest.mark.parametrize("name", ["small_noq", "small_q", "config2_small"])
+@pytest.mark.parametrize("name", ["small_noq", "small_q", "config2_small", "tall"])
 def test_solve_parity_small(models, name):
     p = HPRSOCP_parameters(verbose=False, stoptol=1e-6, max_iter=100000)
     o, g = _pair(models[name])
