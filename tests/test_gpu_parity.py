@@ -186,3 +186,22 @@ def test_schedules_give_identical_iterates(models, name):
     for mode in ("fused", "auto"):
         for a, b in zip(res[mode], res["engine"]):
             assert np.array_equal(a, b), mode
+
+
+def test_warm_start_parity_and_speed(models):
+    """initial_x / initial_y (HPRSOCP_parameters, src/structs.jl:208-277):
+    the GPU and the oracle take the same warm-started path, and a start at a
+    previous solution converges in fewer iterations."""
+    model = models["config0"]
+    p = HPRSOCP_parameters(verbose=False, stoptol=1e-6, max_iter=100000)
+    o, g = _pair(model)
+    cold = g.solve(p)
+    assert cold.status == "OPTIMAL"
+    pw = HPRSOCP_parameters(verbose=False, stoptol=1e-6, max_iter=100000, initial_x=cold.x, initial_y=cold.y)
+    o2, g2 = _pair(model)
+    rg = g2.solve(pw)
+    ro = o2.solve(pw)
+    assert rg.status == ro.status == "OPTIMAL"
+    assert rg.iter < cold.iter
+    assert abs(rg.iter - ro.iter) <= max(10, ro.iter // 20), (rg.iter, ro.iter)
+    assert abs(rg.primal_obj - ro.primal_obj) <= 1e-6 * max(1.0, abs(ro.primal_obj))
