@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <memory>
 
 #include "hpr_engine.cuh"
 
@@ -405,6 +406,12 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
   if (P->initial_x || P->initial_y) HPR_TRY(launch_initial_points(c, P->initial_x, P->initial_y));
   // small problems are launch-bound: replay captured partial iterations
   if (c->A.nnz + c->n + c->m < (int64_t)4000000 && !uses_fused_iterations(c)) HPR_TRY(capture_partial_graph(c, 8));
+  std::unique_ptr<Checkpointer, void (*)(Checkpointer*)> ckpt(nullptr, ckpt_destroy);
+  if (P->auto_save) {
+    int rc = HPR_OK;
+    ckpt.reset(ckpt_create(c, P, &rc));
+    if (rc != HPR_OK) return rc;
+  }
 
   RestartInfo R;
   R.best_sigma = c->sigma;
@@ -432,6 +439,7 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
     if (iter % ci == 0 || print_yes) HPR_TRY(launch_residuals(c, iter == 0, &rs));
     if (rs.KKTx_and_gap_org_bar != rs.KKTx_and_gap_org_bar)
       return set_err(c, HPR_E_NUMERIC, "NaN in the KKT residuals at iteration " + std::to_string(iter));
+    if (ckpt && (iter % ci == 0 || print_yes)) HPR_TRY(ckpt_track(ckpt.get(), iter, c->sigma, rs));
     if (rs.KKTx_and_gap_org_bar < P->stoptol) status = HPR_STATUS_OPTIMAL;
     else if (iter == P->max_iter) status = HPR_STATUS_MAX_ITER;
     else if (now_s() - t0 > P->time_limit) status = HPR_STATUS_TIME_LIMIT;
@@ -464,6 +472,8 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
       std::printf("%5lld    %3.2e    %3.2e    %+7.6e    %+7.6e    %3.2e    %3.2e    %6.2f\n", (long long)iter,
                   rs.err_Rp_org_bar, rs.err_Rd_org_bar, rs.primal_obj_bar, rs.dual_obj_bar, rs.rel_gap_bar, c->sigma,
                   now_s() - t0);
+    // auto-save (algorithm.jl:2871-2880), written behind the iteration
+    if (ckpt && (print_yes || status >= 0)) HPR_TRY(ckpt_save(ckpt.get(), iter, now_s() - t0, c->sigma, rs));
     if (rs.KKTx_and_gap_org_bar < 1e-4 && iter_4 == 0 && time_4 == 0) {
       time_4 = now_s() - t0;
       iter_4 = iter;
@@ -519,6 +529,7 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
     out->last = rs;
     HPR_TRY(launch_unscale(c, out->x, out->y, out->z, out->w));
   }
+  if (ckpt) ckpt_finish(ckpt.get());
   if (P->verbose) print_summary(status, rs, iter, tt, c->upload_s + scaling_s);
   return HPR_OK;
 }
@@ -605,6 +616,8 @@ void hpr_default_params(hpr_params* p) {
   p->lambda_max_Q = -1;
   p->precision = HPR_PREC_FP64;
   p->refine = 0;
+  p->auto_save = 0;
+  p->save_filename = nullptr;  // "HPRSOCP_autosave.npz"
 }
 
 int hpr_create(int device, size_t budget, hpr_ctx** out) {

@@ -247,6 +247,17 @@ int transpose_csr(Ctx* c, const DevCSR& M, DevCSR& T, std::vector<int32_t>& trp)
 // scaling (hpr_scale.cu)
 int run_scaling(Ctx* c, const hpr_params* p, hpr_scale_info* out);
 
+// auto-save of the current and best iterates (hpr_checkpoint.cu)
+struct Checkpointer;
+Checkpointer* ckpt_create(Ctx* c, const hpr_params* P, int* rc);
+// best-iterate bookkeeping after a residual check
+int ckpt_track(Checkpointer* k, int64_t iter, double sigma, const hpr_residuals& rs);
+// stage the current and best iterates and hand them to the writer thread
+int ckpt_save(Checkpointer* k, int64_t iter, double elapsed, double sigma, const hpr_residuals& rs);
+// wait for the last file (a failed write is reported as a warning)
+void ckpt_finish(Checkpointer* k);
+void ckpt_destroy(Checkpointer* k);
+
 // host-side start vector for the power iteration (splitmix64 uniform(-1,1)
 // + 1e-8).  The reference uses randn(MersenneTwister(1)) .+ 1e-8
 // (src/utils/eigenvalues.jl:72-76), which has no portable equivalent.

@@ -102,6 +102,7 @@ struct Request {
   int64_t ticket = 0;
   std::unique_ptr<OwnedProblem> prob;
   hpr_params params{};
+  std::string save_filename;  // owned copy of params.save_filename
   double t_submit = 0;
   size_t est = 0;
 };
@@ -167,6 +168,7 @@ struct hpr_server {
       f.res.w = f.w.data();
       r.params.verbose = 0;
       r.params.device_number = device;
+      r.params.save_filename = r.save_filename.empty() ? nullptr : r.save_filename.c_str();
       f.rc = hpr_upload(ctx, &r.prob->p);
       if (f.rc == HPR_OK) f.rc = hpr_solve(ctx, &r.params, &f.res);
       if (f.rc != HPR_OK) f.err = hpr_last_error(ctx);
@@ -246,6 +248,8 @@ int hpr_serve_submit(hpr_server* s, const hpr_problem* prob, const hpr_params* p
   }
   r.params.initial_x = nullptr;  // warm starts are not carried through the queue
   r.params.initial_y = nullptr;
+  if (r.params.save_filename) r.save_filename = r.params.save_filename;
+  r.params.save_filename = nullptr;
   r.t_submit = now_s();
   {
     std::lock_guard<std::mutex> lk(s->mu);

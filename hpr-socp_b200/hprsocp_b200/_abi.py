@@ -82,7 +82,8 @@ class hpr_params(C.Structure):
                 ("use_Pock_Chambolle_scaling", C.c_int32),
                 ("soc_block_scaling_strategy", C.c_int32), ("verbose", C.c_int32),
                 ("initial_x", _dp), ("initial_y", _dp), ("lambda_max_A", C.c_double),
-                ("lambda_max_Q", C.c_double), ("precision", C.c_int32), ("refine", C.c_int32)]
+                ("lambda_max_Q", C.c_double), ("precision", C.c_int32), ("refine", C.c_int32),
+                ("auto_save", C.c_int32), ("save_filename", C.c_char_p)]
 
 
 class hpr_residuals(C.Structure):
@@ -109,6 +110,13 @@ class hpr_scale_info(C.Structure):
     _fields_ = [("b_scale", C.c_double), ("c_scale", C.c_double), ("norm_b", C.c_double),
                 ("norm_c", C.c_double), ("norm_b_org", C.c_double),
                 ("norm_c_org", C.c_double), ("Q_is_diag", C.c_int32)]
+
+
+class hpr_cbf_data(C.Structure):
+    _fields_ = [("m", C.c_int64), ("n", C.c_int64), ("number_eq", C.c_int64),
+                ("number_ineq", C.c_int64), ("A", hpr_csr), ("rhs", _dp), ("c", _dp),
+                ("l", _dp), ("u", _dp), ("soc_con_idx", _lp), ("n_soc_con_idx", C.c_int64),
+                ("soc_var_idx", _lp), ("n_soc_var_idx", C.c_int64), ("obj_constant", C.c_double)]
 
 
 # Every entry point of include/hprsocp_b200.h with its ctypes signature.
@@ -151,6 +159,11 @@ PROTOTYPES = {
     "hpr_serve_stats": (C.c_int, [C.c_void_p, _lp, _lp, C.POINTER(C.c_size_t)]),
     "hpr_serve_last_error": (C.c_char_p, [C.c_void_p]),
     "hpr_serve_destroy": (C.c_int, [C.c_void_p]),
+    "hpr_cbf_read": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "hpr_cbf_last_error": (C.c_char_p, []),
+    "hpr_cbf_data_get": (C.c_int, [C.c_void_p, C.POINTER(hpr_cbf_data)]),
+    "hpr_cbf_problem": (C.c_int, [C.c_void_p, C.POINTER(hpr_problem)]),
+    "hpr_cbf_free": (None, [C.c_void_p]),
 }
 
 _LIB = None

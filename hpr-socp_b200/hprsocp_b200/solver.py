@@ -8,6 +8,7 @@ the parity tests drive step by step.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 from typing import Optional
 
@@ -38,8 +39,10 @@ class HPRSOCP_parameters:
     soc_block_scaling_strategy: str = "phase_taper"
     initial_x: Optional[np.ndarray] = None
     initial_y: Optional[np.ndarray] = None
+    # auto-save: current and best iterates on print iterations and at the end,
+    # as a .npz archive whose member names are the reference's HDF5 paths
     auto_save: bool = False
-    save_filename: str = "HPRSOCP_autosave.h5"
+    save_filename: str = "HPRSOCP_autosave.npz"
     verbose: bool = True
     use_gpu: bool = True
     # extensions: injected eigenvalue bounds and SpMV precision
@@ -87,6 +90,10 @@ class HPRSOCP_parameters:
         p.lambda_max_Q = self.lambda_max_Q
         p.precision = _abi.HPR_PREC[self.precision]
         p.refine = int(self.refine)
+        p.auto_save = int(self.auto_save)
+        fn = os.fsencode(self.save_filename)
+        keep.append(fn)
+        p.save_filename = fn
         self._keep = keep
         return p
 

@@ -90,6 +90,8 @@ struct CParams
     lambda_max_Q::Float64
     precision::Int32
     refine::Int32
+    auto_save::Int32
+    save_filename::Ptr{UInt8}
 end
 
 struct CResiduals
@@ -128,6 +130,23 @@ end
 CResults() = CResults(0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
                       CResiduals(0, 0, 0, 0, 0, 0, 0, 0), C_NULL, C_NULL, C_NULL, C_NULL)
 
+struct CCbfData
+    m::Int64
+    n::Int64
+    number_eq::Int64
+    number_ineq::Int64
+    A::CCSR
+    rhs::Ptr{Float64}
+    c::Ptr{Float64}
+    l::Ptr{Float64}
+    u::Ptr{Float64}
+    soc_con_idx::Ptr{Int64}
+    n_soc_con_idx::Int64
+    soc_var_idx::Ptr{Int64}
+    n_soc_var_idx::Int64
+    obj_constant::Float64
+end
+
 """Diagonal-plus-low-rank quadratic term Q = Diagonal(d) + F'F, applied as an
 operator (the form the library's Q operator supports besides a CSR Q)."""
 struct DiagPlusLowRankQ
@@ -154,12 +173,17 @@ function c_params(params, keep::Vector{Any})
         error("Unsupported soc_block_scaling_strategy=$(params.soc_block_scaling_strategy).")
     precision = hasproperty(params, :precision) ? Int32(params.precision) : Int32(0)
     refine = hasproperty(params, :refine) ? Int32(params.refine) : Int32(0)
+    # the auto-save archive is .npz (member names = the reference's HDF5
+    # paths); the reference's default name "….h5" is mapped to "….npz"
+    fname = endswith(params.save_filename, ".h5") ? params.save_filename[1:end-3] * ".npz" : params.save_filename
+    fbytes = push!(Vector{UInt8}(codeunits(fname)), 0x00)
+    push!(keep, fbytes)
     return CParams(params.stoptol, params.sigma, params.max_iter, params.time_limit, params.check_iter,
                    params.print_frequency, Int32(params.device_number), Int32(params.use_Ruiz_scaling),
                    Int32(params.ruiz_iterations), Int32(params.use_bc_scaling),
                    BC_NORM[params.bc_scaling_norm_type], Int32(params.use_Pock_Chambolle_scaling),
                    Int32(SOC_STRATEGY[params.soc_block_scaling_strategy]), Int32(params.verbose), x0, y0,
-                   -1.0, -1.0, precision, refine)
+                   -1.0, -1.0, precision, refine, Int32(params.auto_save), pointer(fbytes))
 end
 
 function c_problem(model, keep::Vector{Any})
@@ -222,6 +246,37 @@ function optimize(model, params, Results::Type)
     out.status = STATUS[res.status + 1]
     out.x, out.y, out.z, out.w = x, y, z, w
     return out
+end
+
+"""
+    read_cbf(filename; threads = 0)
+
+The reference's `read_cbf` (src/utils/cbf_io.jl:1438-1455) run by the
+library's multi-threaded C++ reader (`hpr_cbf_read`).  Returns the same
+values: `(Q, c, A, b, SOC_con_idx, number_eq, number_ineq, lb, ub,
+SOC_var_idx, obj_constant)` with `A::SparseMatrixCSC{Float64,Int32}`, ready
+for the reference's `build_from_SOCP_data`.
+"""
+function read_cbf(filename::AbstractString; threads::Integer = 0)
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    rc = ccall((:hpr_cbf_read, LIB[]), Cint, (Cstring, Cint, Ref{Ptr{Cvoid}}), filename, Cint(threads), h)
+    rc == 0 || error(unsafe_string(ccall((:hpr_cbf_last_error, LIB[]), Cstring, ())))
+    try
+        d = Ref{CCbfData}()
+        check(ccall((:hpr_cbf_data_get, LIB[]), Cint, (Ptr{Cvoid}, Ref{CCbfData}), h[], d))
+        D = d[]
+        copyv(p::Ptr{T}, k) where {T} = k == 0 ? T[] : copy(unsafe_wrap(Array, p, Int(k)))
+        m, n, nz = Int(D.m), Int(D.n), Int(D.A.nnz)
+        # the CSR arrays of A are the CSC arrays of A' (0-based -> 1-based)
+        At = SparseMatrixCSC{Float64,Int32}(n, m, copyv(D.A.rowptr, m + 1) .+ Int32(1),
+                                            copyv(D.A.colind, nz) .+ Int32(1), copyv(D.A.values, nz))
+        A = copy(transpose(At))
+        return (spzeros(Float64, n, n), copyv(D.c, n), A, copyv(D.rhs, m),
+                Vector{Int}(copyv(D.soc_con_idx, D.n_soc_con_idx)), Int(D.number_eq), Int(D.number_ineq),
+                copyv(D.l, n), copyv(D.u, n), Vector{Int}(copyv(D.soc_var_idx, D.n_soc_var_idx)), D.obj_constant)
+    finally
+        ccall((:hpr_cbf_free, LIB[]), Cvoid, (Ptr{Cvoid},), h[])
+    end
 end
 
 end # module

@@ -157,6 +157,19 @@ typedef struct hpr_params {
                             * 10 x stoptol) or stops improving; refine < 0
                             * keeps the reduced stream to the end.  Residuals,
                             * restart and sigma logic are FP64 throughout.  */
+  /* Auto-save (HPRSOCP_parameters.auto_save / save_filename,
+   * src/structs.jl:244-247, 271-272; written by save_state_to_hdf5!,
+   * src/algorithm.jl:306-421).  When auto_save != 0, every print iteration
+   * and the final iteration write the current and the best iterate (in
+   * original coordinates), their residuals and these parameters to
+   * save_filename (NULL or "": "HPRSOCP_autosave.npz").  The file is a NumPy
+   * .npz archive whose member names are the reference's HDF5 paths
+   * ("current/x_org", "best/KKTx_and_gap", "parameters/stoptol", ...); it
+   * is replaced atomically and written by a background thread while the
+   * iteration continues.  A failed write is a warning (verbose), not an
+   * error.                                                                 */
+  int32_t auto_save;
+  const char* save_filename;
 } hpr_params;
 
 #define HPR_STATUS_OPTIMAL 0
@@ -422,6 +435,47 @@ const char* hpr_serve_last_error(hpr_server* srv);
 /* Stops the slots after their current solves; queued requests are dropped.
  * Poll every ticket you need before destroying the server.                 */
 int hpr_serve_destroy(hpr_server* srv);
+
+/* ------------------------------------------------------------------------ */
+/* CBF ingest (replaces read_cbf, src/utils/cbf_io.jl:1438-1455, with its   */
+/* layout _cbf_prepare_layout, 493-634).  Host code only: no device needed. */
+/* ------------------------------------------------------------------------ */
+typedef struct hpr_cbf hpr_cbf; /* a parsed file; owns every array below  */
+
+/* read_cbf's return values (the inputs of build_from_SOCP_data,
+ * src/utils/builders.jl:24-108), with A as CSR instead of CSC.             */
+typedef struct hpr_cbf_data {
+  int64_t m;            /* rows kept: equalities, inequalities, cone rows  */
+  int64_t n;            /* variables: linear ones, then cone variables     */
+  int64_t number_eq;
+  int64_t number_ineq;
+  hpr_csr A;            /* 0-based CSR; columns ascending, no duplicates,  */
+                        /* no stored zeros                                 */
+  const double* rhs;    /* m: A x >= rhs / == rhs / rhs on the cone rows   */
+  const double* c;      /* n (negated for OBJSENSE MAX)                    */
+  const double* l;      /* n                                               */
+  const double* u;      /* n                                               */
+  const int64_t* soc_con_idx; /* 1-based cone row starts + end sentinel    */
+  int64_t n_soc_con_idx;
+  const int64_t* soc_var_idx; /* 1-based cone variable starts + sentinel   */
+  int64_t n_soc_var_idx;
+  double obj_constant;  /* negated for OBJSENSE MAX                        */
+} hpr_cbf_data;
+
+/* Parse a .cbf file (conic-linear subset: L+, L-, L=, F, Q) with nthreads
+ * host threads (<= 0: all).  HPR_E_BAD_INPUT on a malformed or unsupported
+ * file, with the reference's message in hpr_cbf_last_error().  The result
+ * does not depend on nthreads.                                              */
+int hpr_cbf_read(const char* path, int nthreads, hpr_cbf** out);
+/* Message of this thread's last failed hpr_cbf_read ("" after a success). */
+const char* hpr_cbf_last_error(void);
+/* Views of the parsed arrays (valid until hpr_cbf_free).                  */
+int hpr_cbf_data_get(const hpr_cbf* f, hpr_cbf_data* out);
+/* The same file as a problem for hpr_upload in build_from_SOCP_data's
+ * layout: AL = AU = rhs on equalities, AL = rhs / AU = +inf on
+ * inequalities, soc_rhs = the cone rows' rhs, 0-based cone starts, Q = 0. */
+int hpr_cbf_problem(const hpr_cbf* f, hpr_problem* out);
+void hpr_cbf_free(hpr_cbf* f);
 
 #ifdef __cplusplus
 }

@@ -60,3 +60,35 @@ def test_no_device_is_an_error_not_a_fallback():
     h = C.c_void_p()
     assert lib.hpr_create(0, 0, C.byref(h)) == _abi.HPR_E_CUDA
     assert not h.value
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every ctypes struct has the C struct's size and field offsets
+    (compiled here from include/hprsocp_b200.h)."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++") or shutil.which("cc")
+    if cxx is None:
+        pytest.skip("no C compiler")
+    structs = [_abi.hpr_csr, _abi.hpr_problem, _abi.hpr_params, _abi.hpr_residuals, _abi.hpr_results,
+               _abi.hpr_scale_info, _abi.hpr_cbf_data]
+    lines = ['#include <cstdio>', '#include <cstddef>', f'#include "{HEADER}"', "int main() {"]
+    for st in structs:
+        name = st.__name__
+        lines.append(f'  std::printf("{name} size %zu\\n", sizeof({name}));')
+        for field, _ in st._fields_:
+            lines.append(f'  std::printf("{name} {field} %zu\\n", offsetof({name}, {field}));')
+    lines.append("  return 0;\n}")
+    src = tmp_path / "layout.cpp"
+    src.write_text("\n".join(lines))
+    exe = str(tmp_path / "layout")
+    subprocess.run([cxx, "-o", exe, str(src)], check=True)
+    got = {}
+    for line in subprocess.run([exe], check=True, capture_output=True, text=True).stdout.splitlines():
+        name, field, value = line.split()
+        got[(name, field)] = int(value)
+    for st in structs:
+        name = st.__name__
+        assert got[(name, "size")] == C.sizeof(st), name
+        for field, _ in st._fields_:
+            assert got[(name, field)] == getattr(st, field).offset, (name, field)

@@ -2,6 +2,7 @@
 builder layout of the reference, round trips and the rejected inputs."""
 import json
 import os
+import re
 
 import numpy as np
 import pytest
@@ -136,3 +137,145 @@ def test_model_cbf_on_the_gpu(tmp_path):
     assert r.status == "OPTIMAL"
     assert np.allclose(r.x, [1.5, 2.5, 8.5], atol=1e-4)
     assert abs(r.primal_obj + 8.5) <= 1e-4
+
+
+# ---------------------------------------------------------------------------
+# The library's C++ reader against the Python restatement of the reference's
+# rules (read_cbf_py): identical arrays, bit for bit, on every case below.
+# ---------------------------------------------------------------------------
+from hprsocp_b200.cbf import read_cbf_py  # noqa: E402
+
+
+def _same(a, b):
+    Qa, ca, Aa, ra, cona, eqa, ina, la, ua, vara, ka = a
+    Qb, cb, Ab, rb, conb, eqb, inb, lb, ub, varb, kb = b
+    assert Aa.shape == Ab.shape and Qa.shape == Qb.shape and Qa.nnz == Qb.nnz == 0
+    assert np.array_equal(Aa.indptr, Ab.indptr) and np.array_equal(Aa.indices, Ab.indices)
+    assert np.array_equal(Aa.data.view(np.uint64), Ab.data.view(np.uint64))
+    for x, y in ((ca, cb), (ra, rb), (la, lb), (ua, ub)):
+        assert np.array_equal(np.asarray(x).view(np.uint64), np.asarray(y).view(np.uint64))
+    assert list(cona) == list(conb) and list(vara) == list(varb)
+    assert (eqa, ina) == (eqb, inb) and ka == kb
+
+
+def _write(tmp_path, name, text, newline="\n"):
+    path = str(tmp_path / name)
+    with open(path, "w", newline="") as f:
+        f.write(text.replace("\n", newline))
+    return path
+
+
+TRICKY = """# comment before the header
+VER
+3
+
+OBJSENSE
+  maximise
+ACOORD
+3
+0 0 2.0
+1 1 -1.5e-3
+0 0 1.0
+VAR
+5 3
+L+ 2
+Q 2
+F 1
+CON
+4 3
+L- 1
+Q 2
+F 1
+   # comments between sections are skipped
+ACOORD
+9
+0 1 0.0
+0 2 4.0
+0 2 -4.0
+1 3 1.25
+1 3 2.5
+1 3 -0.75
+2 4 3.0
+3 0 9.0
+2 0 -0.0
+BCOORD
+4
+0 1.0
+1 -2.0
+1 3.0
+3 7.0
+OBJACOORD
+3
+4 1.0
+4 -2.0
+0 0.5
+OBJBCOORD
+1.5
+PSDCON
+0
+INT
+0
+"""
+
+
+@pytest.mark.parametrize("newline", ["\n", "\r\n", "\r"])
+def test_native_reader_matches_the_restatement_on_edge_rules(tmp_path, newline):
+    """Duplicates (three in a row) summed in file order, zero entries and
+    zero sums dropped, later BCOORD/OBJACOORD entries winning, a block read
+    before CON/VAR applied after the others, F rows dropped, MAX, empty PSD
+    and INT sections, comments, and every line ending."""
+    path = _write(tmp_path, "tricky.cbf", TRICKY, newline)
+    py = read_cbf_py(path)
+    for threads in (1, 3, 8):
+        _same(read_cbf(path, threads=threads), py)
+    Q, c, A, rhs, con, n_eq, n_ineq, l, u, var, const = py
+    # new columns: L+ vars 0, 1 and the F var 4 -> 0, 1, 2; Q vars 2, 3 -> 3, 4.
+    # The (0, 0) entries come from the block read before CON/VAR: applied
+    # after the later block, so A[0, 0] = -(2 + 1) on the negated L- row
+    assert A.shape == (3, 5) and A[0, 0] == -3.0
+    assert 3 not in A[0].indices  # 4 - 4 dropped
+    assert A[1, 4] == (1.25 + 2.5) + (-0.75)
+    assert A.nnz == 4  # the F row's entry and the zeros are gone
+    assert rhs[1] == -3.0  # the later BCOORD entry for row 1 wins
+    assert c[2] == 2.0 and c[0] == -0.5 and const == -1.5  # max: negated
+
+
+def test_native_reader_handles_a_file_without_final_newline(tmp_path):
+    path = _write(tmp_path, "nofinal.cbf", "VAR\n2 1\nL+ 2\nCON\n1 1\nL+ 1\nACOORD\n2\n0 0 1.0\n0 1 2.0")
+    _same(read_cbf(path), read_cbf_py(path))
+    assert read_cbf(path)[2].nnz == 2
+
+
+def test_native_reader_is_thread_invariant_on_a_large_file(tmp_path):
+    rng = np.random.default_rng(7)
+    m, n, nnz = 3000, 2500, 300_000
+    rows = rng.integers(0, m, nnz)
+    cols = rng.integers(0, n, nnz)
+    vals = np.round(rng.standard_normal(nnz), 3)
+    vals[rng.random(nnz) < 0.01] = 0.0
+    con = [("L=", 500), ("L-", 700), ("F", 300), ("L+", 500), ("Q", 1000)]
+    var = [("L+", 1000), ("Q", 1000), ("F", 300), ("L-", 200)]
+    path = str(tmp_path / "big.cbf")
+    write_cbf(path, con, var, list(zip(rows, cols, vals)), [(i, 0.5 * i) for i in range(0, m, 3)],
+              [(j, 1.0) for j in range(0, n, 5)], objoffset=1.0)
+    ref = read_cbf(path, threads=1)
+    for threads in (2, 5, 8):
+        _same(read_cbf(path, threads=threads), ref)
+    _same(ref, read_cbf_py(path))
+
+
+@pytest.mark.parametrize("body, message", [
+    ("VAR\n1 1\nL+ 1\nCON\n1 1\nL+ 1\nACOORD\n2\n0 0 1.0\n", "unexpected EOF inside ACOORD"),
+    ("VAR\n1 1\nL+ 1\nCON\n1 1\nL+ 1\nACOORD\n1\n\n", "expected integer token"),
+    ("VAR\n1 1\nL+ 1\nCON\n1 1\nL+ 1\nACOORD\n1\n0 0 x\n", "expected floating-point token"),
+    ("VAR\n1 1\nL+ 1\nCON\n1 1\nL+ 1\nACOORD\n1\n0 3 1.0\n", "ACOORD index out of range"),
+    ("VAR\n1 1\nL+ 1\nCON\n1 1\nL+ 1\nBCOORD\n1\n4 1.0\n", "BCOORD index out of range"),
+    ("VAR\n1 1\nL+ 1\nCON\n1 1\nL+ 1\nOBJSENSE\nsideways\n", "Unsupported CBF objective sense"),
+    ("VAR\n1 1\nL+ 1\nCON\n1 1\nL+ 1\nDCOORD\n2\n", "PSD constraints are not supported."),
+    ("VAR\n1 1\nL+ 1\nCON\n", "unexpected EOF after CON"),
+])
+def test_native_and_restatement_reject_alike(tmp_path, body, message):
+    path = _write(tmp_path, "bad.cbf", body)
+    for reader in (read_cbf, read_cbf_py):
+        with pytest.raises(ValueError, match=re.escape(message)):
+            reader(path)
