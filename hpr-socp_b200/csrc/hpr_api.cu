@@ -473,7 +473,8 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
                   rs.err_Rp_org_bar, rs.err_Rd_org_bar, rs.primal_obj_bar, rs.dual_obj_bar, rs.rel_gap_bar, c->sigma,
                   now_s() - t0);
     // auto-save (algorithm.jl:2871-2880), written behind the iteration
-    if (ckpt && (print_yes || status >= 0)) HPR_TRY(ckpt_save(ckpt.get(), iter, now_s() - t0, c->sigma, rs));
+    if (ckpt && (print_yes || status >= 0))
+      HPR_TRY(ckpt_save(ckpt.get(), iter, now_s() - t0, c->sigma, rs, status >= 0));
     if (rs.KKTx_and_gap_org_bar < 1e-4 && iter_4 == 0 && time_4 == 0) {
       time_4 = now_s() - t0;
       iter_4 = iter;

@@ -17,10 +17,13 @@
 //   * a writer thread waits for that copy and writes the archive to
 //     `<save_filename>.tmp`, then renames it over `save_filename`, so a
 //     reader never sees a half-written file.
-// The solver stream waits (on the device) for the previous copy before it
-// overwrites the staging area, and the host waits for the writer only when
-// the next save comes before the previous file is written.  The call that
-// started the solve returns after the last file is complete.
+// A print iteration that comes while the previous file is still being
+// written is not saved, so auto-save never holds the iteration back (the
+// reference writes every print iteration, synchronously); the final
+// iteration is always saved, and the call that started the solve returns
+// after its file is complete.  The solver stream waits (on the device) for
+// the previous copy before it overwrites the staging area.  The CRC-32 of
+// the archive's vectors are computed on one thread each.
 //
 // The file is a NumPy .npz archive (hpr_npz.h) with the reference's HDF5
 // paths as member names: no HDF5 library is available to this build.
@@ -127,7 +130,7 @@ struct Checkpointer {
   bool has_job = false, busy = false, stop = false;
   Job job;
   std::string write_err;
-  int64_t files = 0;
+  int64_t files = 0, skipped = 0;
 
   Checkpointer(Ctx* ctx, const hpr_params* p) : c(ctx), P(*p) {
     path = (p->save_filename && p->save_filename[0]) ? p->save_filename : "HPRSOCP_autosave.npz";
@@ -187,9 +190,13 @@ struct Checkpointer {
     return HPR_OK;
   }
 
-  int save(int64_t iter, double elapsed, double sigma, const hpr_residuals& rs) {
+  int save(int64_t iter, double elapsed, double sigma, const hpr_residuals& rs, bool final) {
     {
       std::unique_lock<std::mutex> lk(mu);
+      if (!final && (busy || has_job)) {
+        ++skipped;  // the writer is behind: this print iteration is not saved
+        return HPR_OK;
+      }
       cv.wait(lk, [this] { return !busy && !has_job; });
     }
     if (copy_pending) HPR_CUDA(c, cudaStreamWaitEvent(c->stream, copied, 0));
@@ -259,24 +266,47 @@ struct Checkpointer {
     if (!w.open(tmp)) return w.error();
     const double* cur = host;
     const double* bst = host + vec_len();
-    auto vectors = [&](const char* grp, const double* v) {
-      const std::string g = grp;
-      const double* x = v;
-      const double* wv = has_q ? v + n : v;  // w = x without a quadratic term
+    // CRC-32 of the vector members, one thread each
+    struct Vec {
+      const double* p;
+      int64_t n;
+      uint32_t crc;
+    };
+    std::vector<Vec> vecs;
+    auto group = [&](const double* v) {
       const double* z = v + (has_q ? 2 : 1) * n;
-      const double* y = z + n;
-      bool ok = w.add_vector(g + "/x_org", x, n) && w.add_vector(g + "/w_org", wv, n);
-      if (ok && m > 0) ok = w.add_vector(g + "/y_org", y, m);
-      return ok && w.add_vector(g + "/z_org", z, n);
+      vecs.push_back({v, n, 0});                  // x
+      vecs.push_back({has_q ? v + n : v, n, 0});  // w
+      vecs.push_back({z + n, m, 0});              // y
+      vecs.push_back({z, n, 0});                  // z
+    };
+    group(cur);
+    group(bst);
+    if (P.initial_x) vecs.push_back({P.initial_x, n, 0});
+    if (P.initial_y) vecs.push_back({P.initial_y, m, 0});
+    {
+      std::vector<std::thread> crc_threads;
+      for (Vec& v : vecs)
+        crc_threads.emplace_back([&v] {
+          v.crc = NpzWriter::member_crc("<f8", {v.n}, v.p, (size_t)v.n * sizeof(double));
+        });
+      for (auto& t : crc_threads) t.join();
+    }
+    auto vectors = [&](const char* grp, size_t first) {
+      const std::string g = grp;
+      const Vec* v = vecs.data() + first;
+      bool ok = w.add_vector(g + "/x_org", v[0].p, n, &v[0].crc) && w.add_vector(g + "/w_org", v[1].p, n, &v[1].crc);
+      if (ok && m > 0) ok = w.add_vector(g + "/y_org", v[2].p, m, &v[2].crc);
+      return ok && w.add_vector(g + "/z_org", v[3].p, n, &v[3].crc);
     };
     const hpr_residuals& r = j.rs;
     const hpr_residuals& b = j.best.rs;
     bool ok = w.add_i64("current/iteration", j.iter) && w.add_f64("current/time_elapsed", j.elapsed) &&
-              w.add_string("current/timestamp", j.stamp) && vectors("current", cur) &&
+              w.add_string("current/timestamp", j.stamp) && vectors("current", 0) &&
               w.add_f64("current/sigma", j.sigma) && w.add_f64("current/err_Rp", r.err_Rp_org_bar) &&
               w.add_f64("current/err_Rd", r.err_Rd_org_bar) && w.add_f64("current/primal_obj", r.primal_obj_bar) &&
               w.add_f64("current/dual_obj", r.dual_obj_bar) && w.add_f64("current/rel_gap", r.rel_gap_bar) &&
-              w.add_f64("current/KKTx_and_gap", r.KKTx_and_gap_org_bar) && vectors("best", bst) &&
+              w.add_f64("current/KKTx_and_gap", r.KKTx_and_gap_org_bar) && vectors("best", 4) &&
               w.add_f64("best/sigma", j.best.sigma) && w.add_i64("best/iteration", j.best.iter) &&
               w.add_f64("best/err_Rp", b.err_Rp_org_bar) && w.add_f64("best/err_Rd", b.err_Rd_org_bar) &&
               w.add_f64("best/primal_obj", b.primal_obj_bar) && w.add_f64("best/dual_obj", b.dual_obj_bar) &&
@@ -296,8 +326,8 @@ struct Checkpointer {
               w.add_bool("parameters/use_Pock_Chambolle_scaling", P.use_Pock_Chambolle_scaling != 0) &&
               w.add_string("parameters/soc_block_scaling_strategy", soc_strategy_name(P.soc_block_scaling_strategy)) &&
               w.add_bool("parameters/auto_save", true);
-    if (ok && P.initial_x) ok = w.add_vector("parameters/initial_x", P.initial_x, n);
-    if (ok && P.initial_y) ok = w.add_vector("parameters/initial_y", P.initial_y, m);
+    if (ok && P.initial_x) ok = w.add_vector("parameters/initial_x", P.initial_x, n, &vecs[8].crc);
+    if (ok && P.initial_y) ok = w.add_vector("parameters/initial_y", P.initial_y, m, &vecs[P.initial_x ? 9 : 8].crc);
     if (!w.close() || !ok) {
       std::remove(tmp.c_str());
       return w.error().empty() ? std::string("write failed") : w.error();
@@ -348,8 +378,8 @@ Checkpointer* ckpt_create(Ctx* c, const hpr_params* P, int* rc) {
 int ckpt_track(Checkpointer* k, int64_t iter, double sigma, const hpr_residuals& rs) {
   return k->track(iter, sigma, rs);
 }
-int ckpt_save(Checkpointer* k, int64_t iter, double elapsed, double sigma, const hpr_residuals& rs) {
-  return k->save(iter, elapsed, sigma, rs);
+int ckpt_save(Checkpointer* k, int64_t iter, double elapsed, double sigma, const hpr_residuals& rs, bool final) {
+  return k->save(iter, elapsed, sigma, rs, final);
 }
 void ckpt_finish(Checkpointer* k) { k->finish(); }
 void ckpt_destroy(Checkpointer* k) { delete k; }

@@ -252,8 +252,9 @@ struct Checkpointer;
 Checkpointer* ckpt_create(Ctx* c, const hpr_params* P, int* rc);
 // best-iterate bookkeeping after a residual check
 int ckpt_track(Checkpointer* k, int64_t iter, double sigma, const hpr_residuals& rs);
-// stage the current and best iterates and hand them to the writer thread
-int ckpt_save(Checkpointer* k, int64_t iter, double elapsed, double sigma, const hpr_residuals& rs);
+// stage the current and best iterates and hand them to the writer thread;
+// a non-final save is dropped while the previous file is being written
+int ckpt_save(Checkpointer* k, int64_t iter, double elapsed, double sigma, const hpr_residuals& rs, bool final);
 // wait for the last file (a failed write is reported as a warning)
 void ckpt_finish(Checkpointer* k);
 void ckpt_destroy(Checkpointer* k);

@@ -93,29 +93,39 @@ bool NpzWriter::open(const std::string& path) {
   return true;
 }
 
-bool NpzWriter::add_array(const std::string& name, const std::string& descr, const std::vector<int64_t>& shape,
-                          const void* data, size_t bytes) {
-  if (!err_.empty()) return false;
-  // .npy header: magic, version 1.0, little-endian header length, the
-  // dictionary padded with spaces and ended by '\n' to a multiple of 64
+// .npy header: magic, version 1.0, little-endian header length, the
+// dictionary padded with spaces and ended by '\n' to a multiple of 64
+std::string NpzWriter::npy_header(const std::string& descr, const std::vector<int64_t>& shape) {
   std::string dict = "{'descr': '" + descr + "', 'fortran_order': False, 'shape': " + shape_string(shape) + ", }";
   const size_t unpadded = 10 + dict.size() + 1;
   dict.append((64 - unpadded % 64) % 64, ' ');
   dict.push_back('\n');
-  if (dict.size() > 0xFFFF) return fail("npy header too long for " + name);
   std::string hdr = "\x93NUMPY";
   hdr.push_back('\x01');
   hdr.push_back('\x00');
   hdr.push_back((char)(dict.size() & 0xFF));
-  hdr.push_back((char)(dict.size() >> 8));
-  hdr += dict;
+  hdr.push_back((char)((dict.size() >> 8) & 0xFF));
+  return hdr + dict;
+}
+
+uint32_t NpzWriter::member_crc(const std::string& descr, const std::vector<int64_t>& shape, const void* data,
+                               size_t bytes) {
+  const std::string hdr = npy_header(descr, shape);
+  return crc32_update(crc32_update(0, hdr.data(), hdr.size()), data, bytes);
+}
+
+bool NpzWriter::add_array(const std::string& name, const std::string& descr, const std::vector<int64_t>& shape,
+                          const void* data, size_t bytes, const uint32_t* crc) {
+  if (!err_.empty()) return false;
+  const std::string hdr = npy_header(descr, shape);
+  if (hdr.size() - 10 > 0xFFFF) return fail("npy header too long for " + name);
 
   Entry e;
   e.name = name + ".npy";
   e.size = hdr.size() + bytes;
   e.offset = pos_;
   e.zip64 = force_zip64_ || e.size >= k32Max;
-  e.crc = crc32_update(crc32_update(0, hdr.data(), hdr.size()), data, bytes);
+  e.crc = crc ? *crc : crc32_update(crc32_update(0, hdr.data(), hdr.size()), data, bytes);
 
   unsigned char lh[30];
   auto w16 = [](unsigned char* p, uint32_t v) {
@@ -161,8 +171,8 @@ bool NpzWriter::add_string(const std::string& name, const std::string& s) {
   for (size_t i = 0; i < s.size(); ++i) u[i] = (unsigned char)s[i];
   return add_array(name, "<U" + std::to_string(len), {}, u.data(), u.size() * sizeof(uint32_t));
 }
-bool NpzWriter::add_vector(const std::string& name, const double* v, int64_t n) {
-  return add_array(name, "<f8", {n}, v, (size_t)n * sizeof(double));
+bool NpzWriter::add_vector(const std::string& name, const double* v, int64_t n, const uint32_t* crc) {
+  return add_array(name, "<f8", {n}, v, (size_t)n * sizeof(double), crc);
 }
 
 bool NpzWriter::close() {

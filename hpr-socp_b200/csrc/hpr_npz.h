@@ -34,13 +34,19 @@ class NpzWriter {
   bool open(const std::string& path);
   // One .npy member: `descr` is the NumPy type string ("<f8", "<i8", "|b1",
   // "<U12"), `shape` empty for a 0-d array, `data` the C-ordered elements.
+  // `crc`, when given, is member_crc() of the same arguments (computed
+  // beforehand, for example on another thread).
   bool add_array(const std::string& name, const std::string& descr, const std::vector<int64_t>& shape,
-                 const void* data, size_t bytes);
+                 const void* data, size_t bytes, const uint32_t* crc = nullptr);
+  // The .npy header of a member, and the CRC-32 of header and data.
+  static std::string npy_header(const std::string& descr, const std::vector<int64_t>& shape);
+  static uint32_t member_crc(const std::string& descr, const std::vector<int64_t>& shape, const void* data,
+                             size_t bytes);
   bool add_f64(const std::string& name, double v);
   bool add_i64(const std::string& name, int64_t v);
   bool add_bool(const std::string& name, bool v);
   bool add_string(const std::string& name, const std::string& s);  // ASCII -> '<U{len}'
-  bool add_vector(const std::string& name, const double* v, int64_t n);
+  bool add_vector(const std::string& name, const double* v, int64_t n, const uint32_t* crc = nullptr);
   // Writes the central directory and closes the file.
   bool close();
   const std::string& error() const { return err_; }
