@@ -111,6 +111,69 @@ __device__ void block_reduce(Red& r, double (*s_red)[kThreads / 32]) {
   }
 }
 
+// Cache operators of the engine's loads (defaults measured best on B200:
+// gathers through L2 only, streams and epilogue inputs evict-first):
+//   gathers of xin:      0 ld.global.nc, 1 ld.global.cg (L2 only),
+//                        2 ld.global.nc.L1::no_allocate;
+//   col / val streams:   0 ld.global.cs, 1 ld.global.cg,
+//                        2 ld.global.nc.L1::no_allocate with an L2 evict-first
+//                          policy, 3 ld.global.nc;
+//   epilogue inputs:     0 ld.global.cs, 1 ld.global.cg.
+#ifndef HPR_ENGINE_GATHER
+#define HPR_ENGINE_GATHER 1
+#endif
+#ifndef HPR_ENGINE_STREAM
+#define HPR_ENGINE_STREAM 0
+#endif
+#ifndef HPR_ENGINE_EPILOAD
+#define HPR_ENGINE_EPILOAD 0
+#endif
+
+// ---- loads with the cache operators chosen above
+__device__ __forceinline__ double ld_nc_na(const double* p) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_nc_na(const float* p) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ int32_t ld_stream_pol(const int32_t* p, uint64_t pol) {
+  int32_t v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_stream_pol(const double* p, uint64_t pol) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+template <class T>
+__device__ __forceinline__ T ld_gather(const T* p) {
+  if constexpr (HPR_ENGINE_GATHER == 1) return __ldcg(p);
+  else if constexpr (HPR_ENGINE_GATHER == 2) return ld_nc_na(p);
+  else return __ldg(p);
+}
+template <class T>
+__device__ __forceinline__ T ld_stream(const T* p, uint64_t pol) {
+  if constexpr (HPR_ENGINE_STREAM == 1) return __ldcg(p);
+  else if constexpr (HPR_ENGINE_STREAM == 2) return ld_stream_pol(p, pol);
+  else if constexpr (HPR_ENGINE_STREAM == 3) return __ldg(p);
+  else return __ldcs(p);
+}
+template <class T>
+__device__ __forceinline__ T ld_epi(const T* p) {
+  if constexpr (HPR_ENGINE_EPILOAD == 1) return __ldcg(p);
+  else return __ldcs(p);
+}
+
 // The epilogue inputs of one row, read by `in(k, i)` like a vector.
 template <int NS>
 struct Vals {
@@ -125,7 +188,7 @@ __device__ __forceinline__ void load_vals(Vals<Epi::kSlots>& o, const Epi& epi, 
 #pragma unroll
   for (int k = 0; k < Epi::kSlots; ++k) {
     const double* p = cone ? epi.cone_src[k] : epi.lin_src[k];
-    o.v[k] = p ? __ldcs(p + i) : 0.0;
+    o.v[k] = p ? ld_epi(p + i) : 0.0;
   }
 }
 
@@ -171,10 +234,16 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #ifndef HPR_ENGINE_PIPE
 #define HPR_ENGINE_PIPE 1  // next round's col/val requested before this round's gathers
 #endif
+#ifndef HPR_ENGINE_SUM_UNROLL
+#define HPR_ENGINE_SUM_UNROLL 0  // unrolling of the serial row sums (0: the compiler's choice)
+#endif
+
 constexpr int kWarpsPerCta = HPR_ENGINE_WARPS;
 constexpr int kEngineThreads = kWarpsPerCta * 32;
 constexpr int kGrab = 1;  // tiles taken per atomic
 constexpr int kChunk = HPR_ENGINE_CHUNK;  // elements per lane per gather round
+constexpr int kSumUnroll = HPR_ENGINE_SUM_UNROLL > 0 ? HPR_ENGINE_SUM_UNROLL : 1;
+
 constexpr bool kTwoRows = kRowCap > 32;   // a lane owns rows lane and lane + 32
 
 struct WarpSmem {
@@ -246,6 +315,7 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
   const int nrows = t.re - t.rb;
   const int nnz = t.nze - t.nzb;
   const bool cone = tile_is_cone(t, Epi::kCones);
+  const uint64_t pol = HPR_ENGINE_STREAM == 2 ? l2_evict_first_policy() : 0;
 
   // ---- 0. row pointers and epilogue inputs of this lane's two rows
   int r0b = 0, r0e = 0, r1b = 0, r1e = 0;
@@ -274,8 +344,8 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
         cc[k] = 0;
         vv[k] = 0.0;
         if (e < nnz) {
-          cc[k] = __ldcs(a.M.col + t.nzb + e);
-          if constexpr (PREC == HPR_PREC_FP64) vv[k] = __ldcs(a.M.val + t.nzb + e);
+          cc[k] = ld_stream(a.M.col + t.nzb + e, pol);
+          if constexpr (PREC == HPR_PREC_FP64) vv[k] = ld_stream(a.M.val + t.nzb + e, pol);
           else vv[k] = (double)ldval32<PREC>(a.M, (int64_t)t.nzb + e);
         }
       }
@@ -292,10 +362,10 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
         const int e = c0 + lane + 32 * k;
         if (e < nnz) {
           if constexpr (PREC == HPR_PREC_FP64)
-            ws.prod[e] = vals[k] * (kCoherent ? __ldcg(a.xin + cols[k]) : __ldg(a.xin + cols[k]));
+            ws.prod[e] = vals[k] * (kCoherent ? __ldcg(a.xin + cols[k]) : ld_gather(a.xin + cols[k]));
           else
             ws.prod[e] =
-                (double)((float)vals[k] * (kCoherent ? __ldcg(a.xin32 + cols[k]) : __ldg(a.xin32 + cols[k])));
+                (double)((float)vals[k] * (kCoherent ? __ldcg(a.xin32 + cols[k]) : ld_gather(a.xin32 + cols[k])));
         }
       }
       if (!HPR_ENGINE_PIPE && c0 + 32 * kChunk < nnz) load_round(c0 + 32 * kChunk, ncols, nvals);
@@ -364,6 +434,9 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
   if (lane < nrows) {
     if (r0e - r0b <= kSerialMax) {
       double s = 0.0;
+#if HPR_ENGINE_SUM_UNROLL > 0
+#pragma unroll kSumUnroll
+#endif
       for (int k = r0b; k < r0e; ++k) s = s + ws.prod[k];
       ws.acc[lane] = s;
     } else {
@@ -373,6 +446,9 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
   if (kTwoRows && lane + 32 < nrows) {
     if (r1e - r1b <= kSerialMax) {
       double s = 0.0;
+#if HPR_ENGINE_SUM_UNROLL > 0
+#pragma unroll kSumUnroll
+#endif
       for (int k = r1b; k < r1e; ++k) s = s + ws.prod[k];
       ws.acc[lane + 32] = s;
     } else {
