@@ -7,13 +7,14 @@
 // kRowCap rows.
 //
 // Every warp works on its own tiles with no CTA-wide synchronisation, so the
-// SM's 32+ resident warps hide each other's memory latency.  Persistent
+// SM's 24 resident warps hide each other's memory latency.  Persistent
 // warps take tiles (kGrab at a time) from an atomic counter; per tile a warp
-//   0. loads its rows' row pointers and epilogue inputs into registers (two
-//      rows per lane) so their DRAM latency overlaps the gather phase;
+//   0. loads its rows' row pointers (two rows per lane) into registers;
 //   1. streams the tile's column indices and values with coalesced
-//      evict-first loads, gathers xin through L2 and writes the products to a
-//      warp-private shared-memory buffer;
+//      evict-first loads, gathers xin through L2 (ld.global.cg) and writes the
+//      products to a warp-private shared-memory buffer, then requests the
+//      rows' epilogue inputs (HPR_ENGINE_PREFETCH=1 requests them in step 0,
+//      which costs registers during the gathers);
 //   2. sums each row from shared memory in ascending column order by one
 //      lane (rows of at most kSerialMax nonzeros — bit-identical to the
 //      reference's sequential sparse product) or by the whole warp;
@@ -226,7 +227,7 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #define HPR_ENGINE_CHUNK 2
 #endif
 #ifndef HPR_ENGINE_PREFETCH
-#define HPR_ENGINE_PREFETCH 1  // epilogue inputs loaded before the gather rounds
+#define HPR_ENGINE_PREFETCH 0  // 1: epilogue inputs loaded before the gather rounds
 #endif
 #ifndef HPR_ENGINE_EARLYGRAB
 #define HPR_ENGINE_EARLYGRAB 0

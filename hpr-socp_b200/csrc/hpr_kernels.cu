@@ -9,6 +9,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 
 #include "hpr_engine.cuh"
@@ -841,16 +842,34 @@ FStage<E> fstage(Ctx* c, const DevCSR& M, const Plan& p, const int32_t* cs, cons
   return s;
 }
 
+// The single-CTA kernels use the engine's per-warp buffers (kEngineSmem);
+// above 48 KB a kernel needs the opt-in attribute, set once per kernel.
+constexpr int kSmemOptinMax = 227 * 1024;
+template <class K>
+int allow_engine_smem(Ctx* c, K kernel) {
+  if (kEngineSmem <= 48 * 1024) return HPR_OK;
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;  // (device, kernel)
+  const std::pair<int, const void*> key(c->device, (const void*)kernel);
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count(key)) return HPR_OK;
+  HPR_CUDA(c, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kEngineSmem));
+  done.insert(key);
+  return HPR_OK;
+}
+
 template <class E0, class E1, class E2, class E3>
 int launch_fused_prec(Ctx* c, const FStage<E0>& s0, const FStage<E1>& s1, const FStage<E2>& s2, const FStage<E3>& s3,
                       int iters, int full_last) {
   const int prec = c->precision;
   auto go = [&](auto kernel) {
+    HPR_TRY(allow_engine_smem(c, kernel));
     kernel<<<1, kEngineThreads, kEngineSmem, c->stream>>>(s0, s1, s2, s3, c->d_state, iters, full_last);
+    return HPR_OK;
   };
-  if (prec == HPR_PREC_FP32 && s0.a.M.val32) go(fused_kernel<E0, E1, E2, E3, HPR_PREC_FP32>);
-  else if (prec == HPR_PREC_BF16 && s0.a.M.val16) go(fused_kernel<E0, E1, E2, E3, HPR_PREC_BF16>);
-  else go(fused_kernel<E0, E1, E2, E3, HPR_PREC_FP64>);
+  if (prec == HPR_PREC_FP32 && s0.a.M.val32) HPR_TRY(go(fused_kernel<E0, E1, E2, E3, HPR_PREC_FP32>));
+  else if (prec == HPR_PREC_BF16 && s0.a.M.val16) HPR_TRY(go(fused_kernel<E0, E1, E2, E3, HPR_PREC_BF16>));
+  else HPR_TRY(go(fused_kernel<E0, E1, E2, E3, HPR_PREC_FP64>));
   c->launches++;
   HPR_CUDA(c, cudaGetLastError());
   return HPR_OK;
@@ -862,7 +881,7 @@ bool fused_eligible(const Ctx* c) {
   if (!fits(c->planX) || !fits(c->planY)) return false;
   // with Q the reduced-precision streams apply to A only; keep those unfused
   if (c->has_q && (!fits(c->planQ) || c->precision != HPR_PREC_FP64)) return false;
-  return kEngineSmem <= 48 * 1024;
+  return kEngineSmem <= kSmemOptinMax;
 }
 
 // k iterations (the last one full when full_last) in one launch.
@@ -1350,6 +1369,7 @@ int power_fused_A(Ctx* c, int maxit, double tol, double* lam) {
   HPR_CUDA(c, cudaMemcpyAsync(c->pz, hz.data(), c->m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   auto sat = fstage(c, c->AT, c->planX, c->d_var_start, c->pq, nullptr, plain(c->ptq), plain(c->ptq), true);
   auto sa = fstage(c, c->A, c->planY, c->d_con_start, c->ptq, nullptr, plain(c->pz), plain(c->pz), true);
+  HPR_TRY(allow_engine_smem(c, fused_power_kernel));
   fused_power_kernel<<<1, kEngineThreads, kEngineSmem, c->stream>>>(sat, sa, c->pz, c->pq, c->m, maxit, tol,
                                                                      c->d_red_out + 40);
   c->launches++;
@@ -1444,7 +1464,7 @@ int launch_power_A(Ctx* c, int maxit, double tol, double* lam) {
     return HPR_OK;
   }
   auto small = [](const Plan& p) { return (int64_t)p.tasks.size() <= kFusedMaxTiles; };
-  if (small(c->planX) && small(c->planY) && kEngineSmem <= 48 * 1024) return power_fused_A(c, maxit, tol, lam);
+  if (small(c->planX) && small(c->planY) && kEngineSmem <= kSmemOptinMax) return power_fused_A(c, maxit, tol, lam);
   return power_two_pass_A(c, maxit, tol, lam);
 }
 

@@ -310,9 +310,9 @@ int hpr_compute_residuals(hpr_ctx* ctx, int include_bounds,
  *
  * Limits and rules:
  *  - the problem's tile plan must fit the 2 MiB: at most 32,765 reduction
- *    slots per matrix side (one per 512-nonzero tile, split cone and long
- *    row: about 16M nonzeros); larger problems get HPR_E_UNSUPPORTED with
- *    the sizes in hpr_last_error;
+ *    slots per matrix side (one per tile of at most 704 nonzeros and 64
+ *    rows, split cone and long row: about 20M nonzeros); larger problems
+ *    get HPR_E_UNSUPPORTED with the sizes in hpr_last_error;
  *  - FP64 stream only (HPR_E_UNSUPPORTED after hpr_set_precision != 0);
  *  - nothing in the scratch has to start at zero: every slot is written
  *    before it is read, and no state survives between calls;

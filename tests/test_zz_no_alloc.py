@@ -56,7 +56,7 @@ def test_matches_existing_entry_point_on_two_calls(name, bounds):
 
 
 def test_problem_beyond_the_static_scratch_is_refused():
-    model = instances.config1(1, scale=0.75)  # ~37k tiles per side > 32,765 slots
+    model = instances.config1(1)  # ~36k tiles per side > 32,765 slots
     with Context(model) as ctx:
         ctx.scale(HPRSOCP_parameters(verbose=False))
         with pytest.raises(_abi.HPRError, match="static scratch holds 2097152") as e:
