@@ -424,7 +424,12 @@ def main():
                "what": "hpr_optimize from host arrays: upload + scaling + power iteration + "
                        f"{r.iter} iterations (checks every 150) + unscaled solution read-back; "
                        "inputs are copied once per solve, so bytes per step = bytes per solve / iterations",
-               "seconds": dt}
+               "seconds": dt,
+               # where the call's time went: the HPR loop (power iteration
+               # included, as in the reference's solve time) and the rest
+               # (upload, scaling, unscaled read-back)
+               "phases_s": {"power_iteration": r.power_time, "hpr_loop_after_power": r.time - r.power_time,
+                            "upload_scaling_readback": dt - r.time}}
 
     if rank != 0:
         if dist is not None:

@@ -224,7 +224,7 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #define HPR_ENGINE_MINB 3
 #endif
 #ifndef HPR_ENGINE_CHUNK
-#define HPR_ENGINE_CHUNK 2
+#define HPR_ENGINE_CHUNK 3
 #endif
 #ifndef HPR_ENGINE_PREFETCH
 #define HPR_ENGINE_PREFETCH 0  // 1: epilogue inputs loaded before the gather rounds
@@ -534,8 +534,30 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
 
 constexpr int kEngineSmem = kWarpsPerCta * (int)sizeof(WarpSmem);
 
+// Shared-memory carveout of every engine kernel, in percent of the 228 KB
+// shared-memory maximum: room for exactly HPR_ENGINE_MINB CTAs (with the
+// 1 KB each CTA reserves), so the rest of the SM's 256 KB stays L1.  The
+// kernel needs that L1 (the in-flight gathers and streams land there):
+// left to the driver, epilogues light enough on registers for a fourth CTA
+// get a 228 KB carveout and run a third slower.
+#ifndef HPR_ENGINE_CARVEOUT
+#define HPR_ENGINE_CARVEOUT (((HPR_ENGINE_MINB) * (kEngineSmem + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024))
+#endif
+
+// CTAs per SM requested from the register allocator, and nonzeros per lane
+// per gather round, per epilogue (an epilogue specialises these where its
+// registers call for it).
+template <class Epi>
+struct EngineMinBlocks {
+  static constexpr int value = HPR_ENGINE_MINB;
+};
+template <class Epi>
+struct EngineChunk {
+  static constexpr int value = kChunk;
+};
+
 template <class Epi, int PREC>
-__global__ void __launch_bounds__(kEngineThreads, HPR_ENGINE_MINB) engine_kernel(EngineArgs a, Epi epi) {
+__global__ void __launch_bounds__(kEngineThreads, EngineMinBlocks<Epi>::value) engine_kernel(EngineArgs a, Epi epi) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem* s_ws = reinterpret_cast<WarpSmem*>(smem_raw);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -550,7 +572,8 @@ __global__ void __launch_bounds__(kEngineThreads, HPR_ENGINE_MINB) engine_kernel
     // processed, so its atomic latency is hidden behind the tiles
     int next = 0;
     if (HPR_ENGINE_EARLYGRAB && lane == 0) next = atomicAdd(a.pv.task_ctr, kGrab);
-    for (int q = 0; q < kGrab && base + q < ntasks; ++q) process_warp_tile<Epi, PREC>(a, epi, base + q, ws);
+    for (int q = 0; q < kGrab && base + q < ntasks; ++q)
+      process_warp_tile<Epi, PREC, false, EngineChunk<Epi>::value>(a, epi, base + q, ws);
     if (!HPR_ENGINE_EARLYGRAB && lane == 0) next = atomicAdd(a.pv.task_ctr, kGrab);
     base = __shfl_sync(0xffffffffu, next, 0);
   }
@@ -586,7 +609,19 @@ __global__ void __launch_bounds__(kThreads) final_reduce_kernel(const double* __
   __shared__ double s_red[kMaxRed][kThreads / 32];
   Red r;
   red_init<NRED, MASK>(r);
-  for (int s = threadIdx.x; s < nslots; s += kThreads) {
+  // each thread combines slots threadIdx.x, +kThreads, ... in that order;
+  // four slots' loads are issued before they are combined
+  int s = threadIdx.x;
+  for (; s + 3 * kThreads < nslots; s += 4 * kThreads) {
+    Red o[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int k = 0; k < NRED; ++k) o[u].v[k] = slots[(int64_t)(s + u * kThreads) * kMaxRed + k];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) red_combine<NRED, MASK>(r, o[u]);
+  }
+  for (; s < nslots; s += kThreads) {
     Red o;
 #pragma unroll
     for (int k = 0; k < NRED; ++k) o.v[k] = slots[(int64_t)s * kMaxRed + k];

@@ -143,6 +143,13 @@ struct EpiY {
     finish(i, in(0, i), in(1, i), yb, sp);
   }
 };
+#ifndef HPR_ENGINE_MINB_Y
+#define HPR_ENGINE_MINB_Y HPR_ENGINE_MINB
+#endif
+template <>
+struct EngineMinBlocks<EpiY> {
+  static constexpr int value = HPR_ENGINE_MINB_Y;
+};
 
 // ---------------------------------------------------------------------------
 // Q path, x/w half-step: unified_update_zxw1_kernel_full!/partial!
@@ -209,6 +216,12 @@ struct EpiQX {
     }
     finish(i, in, in(0, i), xb, zr);
   }
+};
+// (the Q path's x-step holds more state per row: two nonzeros per lane per
+// round keep it from spilling)
+template <>
+struct EngineChunk<EpiQX> {
+  static constexpr int value = kChunk < 2 ? kChunk : 2;
 };
 
 // tempv = x_hat + sigma (Qw - Q w_bar): compute_tempv_unified_kernel!
@@ -517,6 +530,8 @@ int engine_grid(int* smem_bytes) {
   std::call_once(once, [] {
     auto k = engine_kernel<Epi, PREC>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    if (HPR_ENGINE_CARVEOUT >= 0)
+      cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, (int)(HPR_ENGINE_CARVEOUT));
     int per_sm = 0, dev = 0, sms = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kEngineThreads, dyn);
     cudaGetDevice(&dev);
