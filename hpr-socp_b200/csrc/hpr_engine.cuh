@@ -235,6 +235,9 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #ifndef HPR_ENGINE_PIPE
 #define HPR_ENGINE_PIPE 1  // next round's col/val requested before this round's gathers
 #endif
+#ifndef HPR_ENGINE_BIGCONE_UNROLL
+#define HPR_ENGINE_BIGCONE_UNROLL 8  // raw values in flight per lane in a split cone's norm
+#endif
 #ifndef HPR_ENGINE_SUM_UNROLL
 #define HPR_ENGINE_SUM_UNROLL 0  // unrolling of the serial row sums (0: the compiler's choice)
 #endif
@@ -265,10 +268,19 @@ __device__ void finalize_big_cone(const EngineArgs& a, Epi& epi, int slot) {
   const double* raw = a.pv.raw;
   const int lane = threadIdx.x & 31;
   __threadfence();
+  // One warp runs over the whole cone (thousands of rows), so for the norm
+  // each lane requests kU raw values before adding them (still in ascending
+  // order).  The projection keeps one row per lane in flight: more would
+  // cost the kernel registers.
+  constexpr int kU = HPR_ENGINE_BIGCONE_UNROLL;
   double part = 0.0;
-  for (int r = bc.rb + 1 + lane; r < bc.re; r += 32) {
-    double v = __ldcg(raw + r);
-    part = part + v * v;
+  for (int r = bc.rb + 1 + lane; r < bc.re; r += 32 * kU) {
+    double v[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) v[u] = (r + 32 * u < bc.re) ? __ldcg(raw + r + 32 * u) : 0.0;
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
+      if (r + 32 * u < bc.re) part = part + v[u] * v[u];
   }
   double ns = sqrt(warp_sum_bcast(part));
   double t = __ldcg(raw + bc.rb);
