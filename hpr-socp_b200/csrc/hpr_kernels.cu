@@ -1436,38 +1436,57 @@ int power_generic(Ctx* c, int64_t len, bool isA, int maxit, double tol, double* 
 // q = z/|z| is folded into the first product (tq = A'z / |z|), and
 // lambda = <q, znew> = <z, znew>/|z| and |znew - lambda q|^2 =
 // |znew|^2 - lambda^2 come from reductions in the second product's
-// epilogue, so an iteration is two engine launches, one reduction finish
-// and one read-back.  Same steps and stopping rule as power_generic.
+// epilogue, so an iteration is two engine launches and one reduction
+// finish; the host reads the results once per batch of iterations.  Same
+// steps and stopping rule as power_generic.
 int power_two_pass_A(Ctx* c, int maxit, double tol, double* lam) {
   const int64_t m = c->m;
   std::vector<double> hz(m);
   power_start_vector(hz, 1);
   double* zb[2] = {c->pz, c->pq};
   HPR_CUDA(c, cudaMemcpyAsync(zb[0], hz.data(), m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  // Result lanes: kBase holds |z|^2 entering a batch; iteration j of the
+  // batch leaves |z_new|^2 in kBase+1+2j and <z_old, z_new> in kBase+2+2j.
+  // The host reads a whole batch at once and takes the first iteration that
+  // meets the tolerance; the iterations queued after it change nothing it
+  // reads, so lambda is the one a check after every iteration would give.
+  constexpr int kBatch = 8;
+  constexpr int kBase = 30;
+  static_assert(kBase + 1 + 2 * kBatch <= 64, "result lanes");
   double* out = c->d_red_out;
   const double* zz = zb[0];
-  HPR_TRY(vec_reduce<1, 0>(c, m, DotF{zz, zz}, 30));  // |z0|^2 into out[30]
-  HPR_TRY(fetch_red(c, 31));
-  double nz2 = c->h_red_out[30];
+  HPR_TRY(vec_reduce<1, 0>(c, m, DotF{zz, zz}, kBase));  // |z0|^2
   double lambda = 1.0;
-  int cur = 0;
-  for (int it = 0; it < maxit; ++it) {
-    EpiScale es{};
-    es.out = c->ptq;
-    es.nz2 = out + 30;
-    HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, zb[cur], nullptr, es, false, false, 0));
-    EpiPow ep{};
-    ep.lin_src[0] = ep.cone_src[0] = zb[cur];
-    ep.out = zb[cur ^ 1];
-    HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->ptq, nullptr, ep, false, true, 30));
-    HPR_TRY(fetch_red(c, 32));
-    const double nn2 = c->h_red_out[30], dot = c->h_red_out[31];
-    lambda = dot / std::sqrt(nz2);
-    const double r2 = std::max(nn2 - lambda * lambda, 0.0);
-    const double err = std::sqrt(r2) / (std::sqrt(nn2) + lambda);
-    nz2 = nn2;
-    cur ^= 1;
-    if (err < tol) break;
+  int cur = 0, it = 0;
+  bool done = false;
+  while (!done && it < maxit) {
+    const int nb = std::min(kBatch, maxit - it);
+    for (int j = 0; j < nb; ++j) {
+      EpiScale es{};
+      es.out = c->ptq;
+      es.nz2 = out + (j == 0 ? kBase : kBase + 1 + 2 * (j - 1));
+      HPR_TRY(engine_launch(c, c->AT, c->planX, c->d_var_start, zb[(cur + j) & 1], nullptr, es, false, false, 0));
+      EpiPow ep{};
+      ep.lin_src[0] = ep.cone_src[0] = zb[(cur + j) & 1];
+      ep.out = zb[(cur + j + 1) & 1];
+      HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->ptq, nullptr, ep, false, true, kBase + 1 + 2 * j));
+    }
+    HPR_TRY(fetch_red(c, kBase + 1 + 2 * nb));
+    double nz2 = c->h_red_out[kBase];
+    for (int j = 0; j < nb && !done; ++j) {
+      const double nn2 = c->h_red_out[kBase + 1 + 2 * j], dot = c->h_red_out[kBase + 2 + 2 * j];
+      lambda = dot / std::sqrt(nz2);
+      const double r2 = std::max(nn2 - lambda * lambda, 0.0);
+      const double err = std::sqrt(r2) / (std::sqrt(nn2) + lambda);
+      nz2 = nn2;
+      ++it;
+      if (err < tol) done = true;
+    }
+    cur = (cur + nb) & 1;
+    // the next batch starts from the last |z|^2
+    if (!done)
+      HPR_CUDA(c, cudaMemcpyAsync(out + kBase, out + kBase + 1 + 2 * (nb - 1), sizeof(double),
+                                  cudaMemcpyDeviceToDevice, c->stream));
   }
   *lam = lambda;
   return HPR_OK;
