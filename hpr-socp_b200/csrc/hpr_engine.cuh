@@ -33,6 +33,8 @@
 
 #include "hpr_internal.h"
 
+#include <type_traits>
+
 namespace hpr {
 
 struct Red {
@@ -183,15 +185,26 @@ struct Vals {
 };
 
 // (the source arrays are selected per slot with compile-time indices so the
-// epilogue stays in the kernel-parameter space)
-template <class Epi>
+// epilogue stays in the kernel-parameter space); the first N slots only
+template <class Epi, int N = Epi::kSlots>
 __device__ __forceinline__ void load_vals(Vals<Epi::kSlots>& o, const Epi& epi, bool cone, int64_t i) {
 #pragma unroll
-  for (int k = 0; k < Epi::kSlots; ++k) {
+  for (int k = 0; k < N; ++k) {
     const double* p = cone ? epi.cone_src[k] : epi.lin_src[k];
     o.v[k] = p ? ld_epi(p + i) : 0.0;
   }
 }
+
+// Slots an epilogue's cone_apply reads (Epi::kApplySlots when declared,
+// else all of them).
+template <class Epi, class = void>
+struct ApplySlots {
+  static constexpr int value = Epi::kSlots;
+};
+template <class Epi>
+struct ApplySlots<Epi, std::void_t<decltype(Epi::kApplySlots)>> {
+  static constexpr int value = Epi::kApplySlots;
+};
 
 struct EngineArgs {
   DevCSR M;
@@ -238,6 +251,9 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #ifndef HPR_ENGINE_BIGCONE_UNROLL
 #define HPR_ENGINE_BIGCONE_UNROLL 8  // raw values in flight per lane in a split cone's norm
 #endif
+#ifndef HPR_ENGINE_BIGCONE_APPLY
+#define HPR_ENGINE_BIGCONE_APPLY 1  // rows in flight per lane in a split cone's projection
+#endif
 #ifndef HPR_ENGINE_SUM_UNROLL
 #define HPR_ENGINE_SUM_UNROLL 0  // unrolling of the serial row sums (0: the compiler's choice)
 #endif
@@ -268,10 +284,10 @@ __device__ void finalize_big_cone(const EngineArgs& a, Epi& epi, int slot) {
   const double* raw = a.pv.raw;
   const int lane = threadIdx.x & 31;
   __threadfence();
-  // One warp runs over the whole cone (thousands of rows), so for the norm
-  // each lane requests kU raw values before adding them (still in ascending
-  // order).  The projection keeps one row per lane in flight: more would
-  // cost the kernel registers.
+  // One warp runs over the whole cone (thousands of rows), so each lane
+  // requests several rows before using them: kU raw values for the norm
+  // (still added in ascending order) and kA rows, each with only the inputs
+  // cone_apply reads, for the projection.
   constexpr int kU = HPR_ENGINE_BIGCONE_UNROLL;
   double part = 0.0;
   for (int r = bc.rb + 1 + lane; r < bc.re; r += 32 * kU) {
@@ -286,10 +302,22 @@ __device__ void finalize_big_cone(const EngineArgs& a, Epi& epi, int slot) {
   double t = __ldcg(raw + bc.rb);
   Red red;
   red_init<Epi::kNRed, Epi::kMaxMask>(red);
-  for (int r = bc.rb + lane; r < bc.re; r += 32) {
-    Vals<Epi::kSlots> v;
-    load_vals<Epi>(v, epi, true, r);
-    epi.cone_apply(r, __ldcg(raw + r), t, ns, r == bc.rb, v, red);
+  constexpr int kA = HPR_ENGINE_BIGCONE_APPLY;
+  constexpr int kN = ApplySlots<Epi>::value;
+  for (int r = bc.rb + lane; r < bc.re; r += 32 * kA) {
+    Vals<Epi::kSlots> v[kA];
+    double rv[kA];
+#pragma unroll
+    for (int u = 0; u < kA; ++u) {
+      rv[u] = 0.0;
+      if (r + 32 * u < bc.re) {
+        load_vals<Epi, kN>(v[u], epi, true, r + 32 * u);
+        rv[u] = __ldcg(raw + r + 32 * u);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kA; ++u)
+      if (r + 32 * u < bc.re) epi.cone_apply(r + 32 * u, rv[u], t, ns, r + 32 * u == bc.rb, v[u], red);
   }
   if constexpr (Epi::kNRed > 0) {
     warp_reduce<Epi::kNRed, Epi::kMaxMask>(red);

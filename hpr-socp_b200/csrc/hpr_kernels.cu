@@ -42,6 +42,7 @@ struct EpiX {
   static constexpr int kNRed = 0;
   static constexpr unsigned kMaxMask = 0;
   static constexpr int kSlots = 5;
+  static constexpr int kApplySlots = 2;  // cone_apply reads x, last_x
   using In = Vals<kSlots>;
   const double* lin_src[kSlots];
   const double* cone_src[kSlots];
@@ -97,6 +98,7 @@ struct EpiY {
   static constexpr int kNRed = 0;
   static constexpr unsigned kMaxMask = 0;
   static constexpr int kSlots = 4;
+  static constexpr int kApplySlots = 2;  // cone_apply reads y, last_y
   using In = Vals<kSlots>;
   const double* lin_src[kSlots];
   const double* cone_src[kSlots];
@@ -417,6 +419,7 @@ struct EpiRp {
   static constexpr int kNRed = 5;
   static constexpr unsigned kMaxMask = 0x7;
   static constexpr int kSlots = 5;
+  static constexpr int kApplySlots = 0;  // cone_apply reads no inputs
   using In = Vals<kSlots>;
   const double* lin_src[kSlots];
   const double* cone_src[kSlots];
