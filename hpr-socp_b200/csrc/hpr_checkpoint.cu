@@ -14,8 +14,8 @@
 //     staging area (one map kernel per vector), and a second stream copies
 //     the staging area to pinned host memory while the solver stream runs
 //     on;
-//   * a writer thread waits for that copy and writes the archive to
-//     `<save_filename>.tmp`, then renames it over `save_filename`, so a
+//   * a writer thread waits for that copy and writes the archive to a
+//     temporary file beside it, then renames it over `save_filename`, so a
 //     reader never sees a half-written file.
 // A print iteration that comes while the previous file is still being
 // written is not saved, so auto-save never holds the iteration back (the
@@ -31,7 +31,10 @@
 #include "hpr_internal.h"
 #include "hpr_npz.h"
 
+#include <unistd.h>
+
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -261,7 +264,10 @@ struct Checkpointer {
 
   // one archive with the reference's layout (algorithm.jl:356-418)
   std::string write_file(const Job& j) {
-    const std::string tmp = path + ".tmp";
+    // a name of its own, so solves that share save_filename (for example in
+    // a server) never write the same temporary file
+    static std::atomic<uint64_t> seq{0};
+    const std::string tmp = path + ".tmp" + std::to_string((long long)getpid()) + "." + std::to_string(seq++);
     NpzWriter w;
     if (!w.open(tmp)) return w.error();
     const double* cur = host;

@@ -66,7 +66,7 @@ def test_final_file_is_the_returned_solution(tmp_path):
     assert bool(d["parameters/auto_save"])
     assert str(d["parameters/soc_block_scaling_strategy"]) == "phase_taper"
     assert str(d["parameters/bc_scaling_norm_type"]) == "l2"
-    assert not os.path.exists(path + ".tmp")
+    assert [f for f in os.listdir(tmp_path) if ".tmp" in f] == []
 
 
 def test_best_iterate_is_the_solve_stopped_there(tmp_path):
