@@ -260,7 +260,10 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 
 constexpr int kWarpsPerCta = HPR_ENGINE_WARPS;
 constexpr int kEngineThreads = kWarpsPerCta * 32;
-constexpr int kGrab = 1;  // tiles taken per atomic
+#ifndef HPR_ENGINE_GRAB
+#define HPR_ENGINE_GRAB 1
+#endif
+constexpr int kGrab = HPR_ENGINE_GRAB;  // tiles taken per atomic
 constexpr int kChunk = HPR_ENGINE_CHUNK;  // elements per lane per gather round
 constexpr int kSumUnroll = HPR_ENGINE_SUM_UNROLL > 0 ? HPR_ENGINE_SUM_UNROLL : 1;
 
