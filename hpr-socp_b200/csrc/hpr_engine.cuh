@@ -254,6 +254,9 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #ifndef HPR_ENGINE_BIGCONE_APPLY
 #define HPR_ENGINE_BIGCONE_APPLY 1  // rows in flight per lane in a split cone's projection
 #endif
+#ifndef HPR_ENGINE_PDL
+#define HPR_ENGINE_PDL 1  // engine kernels use programmatic dependent launch (0: plain launches)
+#endif
 #ifndef HPR_ENGINE_SUM_UNROLL
 #define HPR_ENGINE_SUM_UNROLL 0  // unrolling of the serial row sums (0: the compiler's choice)
 #endif
@@ -604,6 +607,11 @@ __global__ void __launch_bounds__(kEngineThreads, EngineMinBlocks<Epi>::value) e
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem* s_ws = reinterpret_cast<WarpSmem*>(smem_raw);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#if HPR_ENGINE_PDL
+  // launched as a programmatic dependent: nothing is read before the
+  // previous kernel in the stream has completed (a no-op otherwise)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
   const int ntasks = a.pv.ntasks;
   epi.setup(a.st);
   WarpSmem& ws = s_ws[wid];
@@ -620,6 +628,10 @@ __global__ void __launch_bounds__(kEngineThreads, EngineMinBlocks<Epi>::value) e
     if (!HPR_ENGINE_EARLYGRAB && lane == 0) next = atomicAdd(a.pv.task_ctr, kGrab);
     base = __shfl_sync(0xffffffffu, next, 0);
   }
+#if HPR_ENGINE_PDL
+  // no more tiles for this warp: the next kernel may start being scheduled
+  asm volatile("griddepcontrol.launch_dependents;");
+#endif
   // ---- last warp: reset the tile counter, advance the Halpern counter
   if (lane == 0) {
     __threadfence();

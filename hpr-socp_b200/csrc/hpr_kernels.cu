@@ -551,7 +551,24 @@ void launch_engine_prec(Ctx* c, int nt, const EngineArgs& a, const Epi& epi) {
   int dyn = 0;
   const int full = engine_grid<Epi, PREC>(&dyn);
   const int g = std::max(1, std::min(full, (nt + kWarpsPerCta - 1) / kWarpsPerCta));
+#if HPR_ENGINE_PDL
+  // programmatic dependent launch: the kernel may be scheduled while the
+  // previous one drains; it waits (griddepcontrol.wait) for that kernel's
+  // completion before its first memory access
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)g);
+  cfg.blockDim = dim3(kEngineThreads);
+  cfg.dynamicSmemBytes = (size_t)dyn;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, engine_kernel<Epi, PREC>, a, epi);
+#else
   engine_kernel<Epi, PREC><<<g, kEngineThreads, dyn, c->stream>>>(a, epi);
+#endif
 }
 
 template <class Epi>
