@@ -254,6 +254,9 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #ifndef HPR_ENGINE_BIGCONE_APPLY
 #define HPR_ENGINE_BIGCONE_APPLY 1  // rows in flight per lane in a split cone's projection
 #endif
+#ifndef HPR_ENGINE_SUM_PAIR
+#define HPR_ENGINE_SUM_PAIR 0  // 1: a lane sums its two rows in one loop
+#endif
 #ifndef HPR_ENGINE_PDL
 #define HPR_ENGINE_PDL 1  // engine kernels use programmatic dependent launch (0: plain launches)
 #endif
@@ -478,6 +481,26 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
   }
   // ---- 2. row sums
   bool long0 = false, long1 = false;
+#if HPR_ENGINE_SUM_PAIR
+  if (kTwoRows) {
+    // the lane's two rows summed in one loop: two independent chains, each
+    // in ascending column order
+    const bool s0 = lane < nrows && r0e - r0b <= kSerialMax;
+    const bool s1 = lane + 32 < nrows && r1e - r1b <= kSerialMax;
+    long0 = lane < nrows && !s0;
+    long1 = lane + 32 < nrows && !s1;
+    const int n0 = s0 ? r0e - r0b : 0, n1 = s1 ? r1e - r1b : 0;
+    const int nmax = n0 > n1 ? n0 : n1;
+    double a0 = 0.0, a1 = 0.0;
+    for (int k = 0; k < nmax; ++k) {
+      if (k < n0) a0 = a0 + ws.prod[r0b + k];
+      if (k < n1) a1 = a1 + ws.prod[r1b + k];
+    }
+    if (s0) ws.acc[lane] = a0;
+    if (s1) ws.acc[lane + 32] = a1;
+  } else
+#endif
+  {
   if (lane < nrows) {
     if (r0e - r0b <= kSerialMax) {
       double s = 0.0;
@@ -501,6 +524,7 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
     } else {
       long1 = true;
     }
+  }
   }
   {
     unsigned m0 = __ballot_sync(0xffffffffu, long0), m1 = kTwoRows ? __ballot_sync(0xffffffffu, long1) : 0u;
