@@ -202,17 +202,6 @@ def run_serving(args):
     stream = instances.serving_stream(11, args.requests, rate=args.rate)
     params = [HPRSOCP_parameters(verbose=False, stoptol=tol, max_iter=200000) for _, tol, _ in stream]
     lib = _abi.load_library()
-    # one at a time: the first `baseline` requests, each a full hpr_optimize
-    nb = min(args.baseline, len(stream))
-    t0 = time.perf_counter()
-    for (model, _, _), p in zip(stream[:nb], params[:nb]):
-        prob, pc = model.to_c(), p.to_c()
-        x, y, z = np.zeros(model.n), np.zeros(model.m), np.zeros(model.n)
-        r = _abi.hpr_results()
-        r.x, r.y, r.z = _abi.dptr(x), _abi.dptr(y), _abi.dptr(z)
-        if lib.hpr_optimize(C.byref(prob), C.byref(pc), C.byref(r)) != 0:
-            raise RuntimeError("hpr_optimize failed")
-    seq_rate = nb / (time.perf_counter() - t0)
     # the server: requests submitted at their arrival times (all at t = 0 at
     # saturation), results polled in submission order
     with Server(slots=args.slots) as srv:
@@ -233,6 +222,24 @@ def run_serving(args):
             ok += r.status == "OPTIMAL"
         wall = time.perf_counter() - t0
     rate = len(stream) / wall
+    # one at a time, after the server (so both run with the CUDA context up
+    # and the schedule autotuner's choices made): the first `baseline`
+    # requests, each a full hpr_optimize, after one untimed solve
+    nb = min(args.baseline, len(stream))
+
+    def solve_one(model, p):
+        prob, pc = model.to_c(), p.to_c()
+        x, y, z = np.zeros(model.n), np.zeros(model.m), np.zeros(model.n)
+        r = _abi.hpr_results()
+        r.x, r.y, r.z = _abi.dptr(x), _abi.dptr(y), _abi.dptr(z)
+        if lib.hpr_optimize(C.byref(prob), C.byref(pc), C.byref(r)) != 0:
+            raise RuntimeError("hpr_optimize failed")
+
+    solve_one(stream[0][0], params[0])
+    t0 = time.perf_counter()
+    for (model, _, _), p in zip(stream[:nb], params[:nb]):
+        solve_one(model, p)
+    seq_rate = nb / (time.perf_counter() - t0)
     lats = np.sort(np.asarray(lats))
     line = {"metric": "solves/s", "value": rate, "unit": "solves/s", "n_gpus": 1, "steps": len(stream),
             "warmup": 2, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -245,7 +252,8 @@ def run_serving(args):
                           "max": float(lats[-1])},
             "optimal": ok, "mean_iterations": float(np.mean(iters)),
             "one_at_a_time": {"value": seq_rate, "unit": "solves/s", "requests": nb,
-                              "how": "hpr_optimize per request, sequentially"},
+                              "how": "hpr_optimize per request, sequentially, after the server run "
+                                     "and one untimed solve"},
             "speedup_vs_one_at_a_time": rate / seq_rate}
     print(json.dumps(line))
 

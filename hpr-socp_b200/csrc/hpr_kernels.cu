@@ -1259,6 +1259,11 @@ int launch_sigma_terms(Ctx* c, double* a, double* b, double* cc, double* d) {
 // unified_golden_Q_diag (unified_operations.jl:411-449): each evaluation is
 // one fused pass over diag(Q), A'dy and Q A'dy.
 namespace {
+// vectors up to this length run the golden-section search in one CTA
+#ifndef HPR_GOLDEN_DEVICE_MAX_N
+#define HPR_GOLDEN_DEVICE_MAX_N 65536
+#endif
+constexpr int64_t kGoldenDeviceMaxN = HPR_GOLDEN_DEVICE_MAX_N;
 struct GoldenF {
   const double *dq, *c, *d;
   double x;
@@ -1266,8 +1271,83 @@ struct GoldenF {
 };
 }  // namespace
 
+namespace {
+// The whole golden-section search of unified_golden_Q_diag in one CTA, for
+// vectors short enough that one CTA reduces them quickly: each evaluation
+// sums the terms in the order of the host-driven search below (chunk j of
+// red_grid(n) as vec_reduce_kernel's CTA j, then the chunk sums as
+// final_reduce_kernel), and thread 0 runs the same interval updates, so the
+// result is the same to the bit without a host round trip per evaluation.
+__global__ void __launch_bounds__(kThreads)
+    golden_diag_kernel(int64_t n, int g, const double* __restrict__ dq, const double* __restrict__ cv,
+                       const double* __restrict__ dv, double a, double b, double lo, double hi, double tol,
+                       int maxiter, double* __restrict__ out) {
+  __shared__ double s_red[kMaxRed][kThreads / 32];
+  __shared__ double s_slot[kRedGrid];
+  __shared__ double s_f;
+  __shared__ int s_go;
+  auto eval = [&](double x) {
+    const int64_t per = (n + g - 1) / g;
+    for (int j = 0; j < g; ++j) {
+      Red r;
+      red_init<1, 0>(r);
+      const int64_t bb = (int64_t)j * per, ee = bb + per < n ? bb + per : n;
+      for (int64_t i = bb + threadIdx.x; i < ee; i += kThreads) r.v[0] = r.v[0] + cv[i] * (dv[i] / (1.0 + x * dq[i]));
+      block_reduce<1, 0>(r, s_red);
+      if (threadIdx.x == 0) s_slot[j] = r.v[0];
+    }
+    __syncthreads();
+    Red r;
+    red_init<1, 0>(r);
+    for (int k = threadIdx.x; k < g; k += kThreads) r.v[0] = r.v[0] + s_slot[k];
+    block_reduce<1, 0>(r, s_red);
+    if (threadIdx.x == 0) s_f = a * x + b / x + x * x * r.v[0];
+    __syncthreads();
+    return s_f;
+  };
+  const double phi = (sqrt(5.0) - 1.0) / 2.0;
+  double x1 = hi - phi * (hi - lo);
+  double x2 = lo + phi * (hi - lo);
+  double f1 = eval(x1);
+  double f2 = eval(x2);
+  int it = 0;
+  while (true) {
+    // every thread holds the same scalars; thread 0 decides for all
+    if (threadIdx.x == 0) s_go = (fabs(hi - lo) > tol * fmax(1.0, fabs(lo)) && it < maxiter) ? 1 : 0;
+    __syncthreads();
+    const int go = s_go;
+    __syncthreads();
+    if (!go) break;
+    if (f1 > f2) {
+      lo = x1;
+      x1 = x2;
+      f1 = f2;
+      x2 = lo + phi * (hi - lo);
+      f2 = eval(x2);
+    } else {
+      hi = x2;
+      x2 = x1;
+      f2 = f1;
+      x1 = hi - phi * (hi - lo);
+      f1 = eval(x1);
+    }
+    it++;
+  }
+  if (threadIdx.x == 0) out[0] = (f1 < f2) ? x1 : x2;
+}
+}  // namespace
+
 int launch_golden_diag(Ctx* c, double a, double b, double lo, double hi, double tol, double* out) {
   const int maxiter = 200;
+  if (c->n > 0 && c->n <= kGoldenDeviceMaxN) {
+    golden_diag_kernel<<<1, kThreads, 0, c->stream>>>(c->n, red_grid(c->n), c->diag_Q, c->ATdy, c->QATdy, a, b, lo, hi,
+                                                      tol, maxiter, c->d_red_out);
+    c->launches++;
+    HPR_CUDA(c, cudaGetLastError());
+    HPR_TRY(fetch_red(c, 1));
+    *out = c->h_red_out[0];
+    return HPR_OK;
+  }
   double phi = (std::sqrt(5.0) - 1.0) / 2.0;
   auto f = [&](double x, double* fx) -> int {
     HPR_TRY(vec_reduce<1, 0>(c, c->n, GoldenF{c->diag_Q, c->ATdy, c->QATdy, x}, 0));
