@@ -10,6 +10,13 @@
 
 #include "hpr_engine.cuh"
 
+#ifndef HPR_SMALL_PLAN_NNZ
+#define HPR_SMALL_PLAN_NNZ 0
+#endif
+#ifndef HPR_SMALL_TILE
+#define HPR_SMALL_TILE 256
+#endif
+
 namespace hpr {
 
 int set_err(Ctx* c, int code, const std::string& msg) {
@@ -762,12 +769,16 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   // plans
   vector<int64_t> vcones = c->h_var_idx.size() > 1 ? c->h_var_idx : vector<int64_t>();
   vector<int64_t> ccones = c->h_con_idx.size() > 1 ? c->h_con_idx : vector<int64_t>();
-  build_plan(trp, n, vcones, c->planX);
-  build_plan(rp, m, ccones, c->planY);
+  // problems below HPR_SMALL_PLAN_NNZ nonzeros get tiles of at most
+  // HPR_SMALL_TILE nonzeros: they occupy few warps, so shorter tiles shorten
+  // each launch's longest chain (0: every problem uses full tiles)
+  const int cap = c->A.nnz < (int64_t)HPR_SMALL_PLAN_NNZ ? (int)HPR_SMALL_TILE : 0;
+  build_plan(trp, n, vcones, c->planX, cap);
+  build_plan(rp, m, ccones, c->planY, cap);
   HPR_TRY(upload_plan(c, c->planX));
   HPR_TRY(upload_plan(c, c->planY));
   if (c->has_q) {
-    build_plan(qrp, n, vcones, c->planQ);
+    build_plan(qrp, n, vcones, c->planQ, cap);
     HPR_TRY(upload_plan(c, c->planQ));
   }
   // problem vectors

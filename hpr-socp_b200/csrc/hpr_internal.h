@@ -85,8 +85,9 @@ struct Plan {
 // Build the task list of one matrix side.  `cone_starts` holds the first row
 // of every cone plus an end sentinel (empty when the side has no cones);
 // rows before cone_starts[0] are linear rows.
+// `nnz_cap` (<= kNnzTile; 0: kNnzTile) caps the nonzeros of a tile.
 void build_plan(const std::vector<int32_t>& rowptr, int64_t nrows,
-                const std::vector<int64_t>& cone_starts, Plan& plan);
+                const std::vector<int64_t>& cone_starts, Plan& plan, int nnz_cap = 0);
 
 struct DevCSR {
   int64_t nrows = 0, ncols = 0, nnz = 0;

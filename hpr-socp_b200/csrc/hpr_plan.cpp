@@ -26,9 +26,9 @@ namespace hpr {
 namespace {
 
 void emit_long_row(const std::vector<int32_t>& rp, int32_t r, int32_t bigslot,
-                   int32_t cone, Plan& plan, std::vector<Task>& out) {
+                   int32_t cone, int32_t cap, Plan& plan, std::vector<Task>& out) {
   int32_t nzb = rp[r], nze = rp[r + 1];
-  int32_t nparts = (nze - nzb + kNnzTile - 1) / kNnzTile;
+  int32_t nparts = (nze - nzb + cap - 1) / cap;
   LongRow lr;
   lr.row = r;
   lr.nparts = nparts;
@@ -41,8 +41,8 @@ void emit_long_row(const std::vector<int32_t>& rp, int32_t r, int32_t bigslot,
     Task t{};
     t.rb = r;
     t.re = r + 1;
-    t.nzb = nzb + p * kNnzTile;
-    t.nze = std::min(nze, t.nzb + kNnzTile);
+    t.nzb = nzb + p * cap;
+    t.nze = std::min(nze, t.nzb + cap);
     t.kind = TASK_LONG_PART;
     t.ncones = 0;
     t.cone = cone;
@@ -55,7 +55,8 @@ void emit_long_row(const std::vector<int32_t>& rp, int32_t r, int32_t bigslot,
 }  // namespace
 
 void build_plan(const std::vector<int32_t>& rp, int64_t nrows,
-                const std::vector<int64_t>& cone_starts, Plan& plan) {
+                const std::vector<int64_t>& cone_starts, Plan& plan, int nnz_cap) {
+  const int32_t cap = (nnz_cap > 0 && nnz_cap < kNnzTile) ? nnz_cap : kNnzTile;
   plan.nrows = nrows;
   plan.tasks.clear();
   plan.big.clear();
@@ -71,8 +72,8 @@ void build_plan(const std::vector<int32_t>& rp, int64_t nrows,
     int64_t start = r, cnt = 0, nz = 0;
     while (r < lin_end && cnt < kRowCap) {
       int64_t rn = (int64_t)rp[r + 1] - rp[r];
-      if (rn > kNnzTile) break;
-      if (nz + rn > kNnzTile && cnt > 0) break;
+      if (rn > cap) break;
+      if (nz + rn > cap && cnt > 0) break;
       nz += rn;
       cnt++;
       r++;
@@ -89,8 +90,8 @@ void build_plan(const std::vector<int32_t>& rp, int64_t nrows,
       t.group = -1;
       rows.push_back(t);
     }
-    if (r < lin_end && (int64_t)rp[r + 1] - rp[r] > kNnzTile) {
-      emit_long_row(rp, (int32_t)r, -1, -1, plan, multi);
+    if (r < lin_end && (int64_t)rp[r + 1] - rp[r] > cap) {
+      emit_long_row(rp, (int32_t)r, -1, -1, cap, plan, multi);
       r++;
     }
   }
@@ -107,11 +108,11 @@ void build_plan(const std::vector<int32_t>& rp, int64_t nrows,
     int64_t a = cone_starts[k], b = cone_starts[k + 1];
     int64_t d = b - a;
     int64_t cnz = (int64_t)rp[b] - rp[a];
-    bool big = d > kSmallConeMax || cnz > kNnzTile;
+    bool big = d > kSmallConeMax || cnz > cap;
     if (d <= 0) continue;
     if (!big) {
       if (open && ((cur.re - cur.rb) + d > kRowCap ||
-                   (int64_t)(cur.nze - cur.nzb) + cnz > kNnzTile ||
+                   (int64_t)(cur.nze - cur.nzb) + cnz > cap ||
                    cur.ncones >= 32000))
         flush();
       if (!open) {
@@ -142,8 +143,8 @@ void build_plan(const std::vector<int32_t>& rp, int64_t nrows,
     int64_t q = a;
     while (q < b) {
       int64_t rn = (int64_t)rp[q + 1] - rp[q];
-      if (rn > kNnzTile) {
-        emit_long_row(rp, (int32_t)q, slot, (int32_t)k, plan, multi);
+      if (rn > cap) {
+        emit_long_row(rp, (int32_t)q, slot, (int32_t)k, cap, plan, multi);
         plan.big[slot].nparts++;
         q++;
         continue;
@@ -151,8 +152,8 @@ void build_plan(const std::vector<int32_t>& rp, int64_t nrows,
       int64_t start = q, cnt = 0, nz = 0;
       while (q < b && cnt < kRowCap) {
         int64_t rq = (int64_t)rp[q + 1] - rp[q];
-        if (rq > kNnzTile) break;
-        if (nz + rq > kNnzTile && cnt > 0) break;
+        if (rq > cap) break;
+        if (nz + rq > cap && cnt > 0) break;
         nz += rq;
         cnt++;
         q++;
