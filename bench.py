@@ -35,14 +35,13 @@ METRIC = "HPR iters/s"
 
 
 def measured_peak():
-    for p in (os.path.join(ROOT, "MEASURED_PEAKS.json"), "/root/repo/MEASURED_PEAKS.json"):
-        try:
-            with open(p) as f:
-                d = json.load(f)
-            return float(d["hbm_gbs"]), "measured"
-        except (OSError, KeyError, ValueError):
-            continue
-    return 6650.0, "fallback"
+    """HBM copy bandwidth measured on this pool's B200s (MEASURED_PEAKS.json
+    beside this file), else the pool's earlier fallback figure."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
 
 
 class ClockSampler:
@@ -60,7 +59,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -72,6 +71,16 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_samples(self, count, timeout=5.0):
+        """Block until `count` more samples than now have arrived (nvidia-smi
+        takes a moment to start), so a short timed region is bracketed."""
+        if not self.proc:
+            return
+        target = len(self.lines) + count
+        t0 = time.perf_counter()
+        while len(self.lines) < target and time.perf_counter() - t0 < timeout and self.proc.poll() is None:
+            time.sleep(0.02)
+
     def __exit__(self, *a):
         if self.proc:
             self.proc.terminate()
@@ -80,10 +89,11 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, first=0):
+        """Median SM clock and the throttle reasons seen in samples[first:]."""
         sm, smax, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[first:]:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -154,38 +164,52 @@ def cpu_iteration_rate(model, iters=3, threads=0):
     return iters / dt
 
 
+def arm_config(args, world=1):
+    """The `config` object both arms print (the driver compares them)."""
+    return {"workload": WORKLOAD, "precision": "fp64", "l2": "inputs larger than L2 (A + A' ~ 600 MB)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU", "scale": args.scale}
+
+
 def run_reference(args, model, budget_s=150.0):
-    """CPU arm: the oracle with every host thread.  Each step is one HPR
-    iteration; the timed loop stops early after ``budget_s`` seconds so the
-    run stays bounded, and the rate is over the iterations it completed."""
+    """CPU arm: the oracle (the CPU restatement of the reference solver) with
+    every host thread, timed over the same phases as the GPU arm's `e2e`:
+    copying the problem in, scaling, the power iteration (tolerance 1e-4,
+    as the reference), K HPR iterations with the residual check every 150
+    iterations, and the unscaled solution read-back.  `value` is the
+    iteration rate of the HPR loop alone, the counterpart of the GPU arm's
+    device-resident rate.  The solve stops at ``budget_s`` seconds (the
+    reference's time_limit rule, which counts the power iteration) so the
+    run stays bounded; the rates are over the iterations it completed."""
     cores = os.cpu_count() or 1
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle_ctx import OracleContext
     from hprsocp_b200 import HPRSOCP_parameters
-    o = OracleContext(model, threads=0)
-    o.scale(HPRSOCP_parameters(verbose=False))
-    o.set_sigma_lambda(1.0, 1.05 * 4000.0, 0.0)
-    for _ in range(args.warmup):
-        o.iterate(1, False)
-    done = 0
+    p = HPRSOCP_parameters(verbose=False, max_iter=args.steps, stoptol=0.0, check_iter=150,
+                           print_frequency=10**9, time_limit=budget_s)
     t0 = time.perf_counter()
-    while done < args.steps:
-        o.iterate(1, done == args.steps - 1)
-        done += 1
-        if time.perf_counter() - t0 > budget_s:
-            break
-    dt = time.perf_counter() - t0
+    o = OracleContext(model, threads=0)
+    r = o.solve(p)  # scaling, power iteration, HPR loop, unscaled solution
+    total = time.perf_counter() - t0
     o.close()
-    v = done / dt
-    sample = f"{done} of {args.steps} HPR iterations of the benchmark instance" + (
-        f" (stopped at the {budget_s:.0f} s bound)" if done < args.steps else "")
+    loop_s = max(r.time - r.power_time, 1e-9)
+    done = max(r.iter, 1)
+    v = done / loop_s
+    sample = f"{r.iter} of {args.steps} HPR iterations of the benchmark instance, one full solve" + (
+        f" (stopped at the {budget_s:.0f} s bound)" if r.iter < args.steps else "")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "iter/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / done,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * loop_s / done,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator, seed 1)",
-            "config": {"workload": WORKLOAD, "path": "CPU restatement of the reference iteration (oracle port)"},
+            "config": arm_config(args, args.gpus),
+            "path": "CPU restatement of the reference solver (oracle port), all host threads; no JIT, so the "
+                    "warm-up steps do not apply",
             "cpu_baseline": {"value": v, "unit": "iter/s", "cores": cores, "kind": "port", "sample": sample},
-            "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": r.iter / total, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                    "seconds": total,
+                    "what": "oracle solve from host arrays: problem copy + scaling + power iteration + "
+                            f"{r.iter} iterations (checks every 150) + unscaled solution",
+                    "phases_s": {"power_iteration": r.power_time, "hpr_loop_after_power": loop_s,
+                                 "setup_scaling_readback": total - r.time}}}
     print(json.dumps(line))
 
 
@@ -393,11 +417,19 @@ def main():
     sigma = info["norm_b"] / info["norm_c"]
     ctx.set_sigma_lambda(sigma, lam, 0.0)
     ctx.set_inner(0)
-    ctx.iterate(args.warmup, False)
-    barrier(dist)
     with ClockSampler(dev) as clk:
+        # clocks are sampled from the warm-up on; a timed region shorter than
+        # the sampling period is followed by untimed iterations until two
+        # samples have been taken under load
+        clk.wait_samples(1)
+        first = len(clk.lines)
+        ctx.iterate(args.warmup, False)
+        barrier(dist)
         ctx.iterate(args.steps, True)  # device-timed with CUDA events inside
-    ms, launches = ctx.last_iterate()
+        ms, launches = ctx.last_iterate()
+        while clk.proc and clk.proc.poll() is None and len(clk.lines) - first < 2:
+            ctx.iterate(20, False)
+    clocks = clk.summary(first)
     ms = dist_max(dist, ms)
     bytes_iter = ctx.iteration_bytes()
     ctx.close()
@@ -463,9 +495,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per_iter_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, seed 1)",
-        "config": {"workload": WORKLOAD, "precision": "fp64", "l2": "inputs larger than L2 (A + A' ~ 600 MB)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "scale": args.scale},
+        "config": arm_config(args, world),
         "hbm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
@@ -474,7 +504,7 @@ def main():
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": int(launches),
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     print(json.dumps(line))
     if dist is not None:

@@ -75,6 +75,12 @@ void free_all(Ctx* c) {
     f(p->d_partials);
     f(p->d_raw);
     f(p->d_ctr);
+    f(p->d_runs);
+    f(p->d_desc);
+    f(p->d_tcol);
+    f(p->d_tval);
+    f(p->d_tval32);
+    f(p->d_tval16);
     *p = Plan();
   }
   double** vs[] = {&c->c,      &c->l,      &c->u,      &c->AL,       &c->AU,     &c->soc_rhs, &c->soc_rhs_full,
@@ -374,6 +380,7 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
     if (P->verbose) std::printf("GPU SCALING time: %.2f seconds\n", scaling_s);
   }
   HPR_TRY(apply_precision(c, P->precision));
+  HPR_TRY(prepare_engine(c));
   // sigma (allocate_workspace, algorithm.jl:1531-1551)
   double sigma = 1.0;
   if (P->sigma == -1) {
@@ -832,8 +839,10 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   c->b_scale = c->c_scale = 1.0;
   c->precision = HPR_PREC_FP64;
   HPR_TRY(push_state(c));
-  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
   c->uploaded = true;
+  // the engine's tiled copies of the matrices (scaling rebuilds them in place)
+  HPR_TRY(prepare_engine(c));
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
   c->scaled = false;
   c->upload_s = now_s() - t_up;
   return HPR_OK;
@@ -992,6 +1001,8 @@ int hpr_set_vector(hpr_ctx* h, int which, const double* host, size_t len) {
     HPR_CUDA(c, cudaMemcpyAsync(p, host, L * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     HPR_CUDA(c, cudaStreamSynchronize(c->stream));
   }
+  if (which == HPR_VEC_A_VALUES) ++c->A.version;
+  if (which == HPR_VEC_AT_VALUES) ++c->AT.version;
   if (which == HPR_VEC_SOC_RHS && L > 0) {
     // the kernels read the row-aligned copy (zero on linear rows)
     HPR_CUDA(c, cudaMemcpyAsync(c->soc_rhs_full + c->m_lin, c->soc_rhs, L * sizeof(double),

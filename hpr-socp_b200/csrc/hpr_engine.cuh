@@ -237,7 +237,7 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #define HPR_ENGINE_MINB 3
 #endif
 #ifndef HPR_ENGINE_CHUNK
-#define HPR_ENGINE_CHUNK 3
+#define HPR_ENGINE_CHUNK 4
 #endif
 #ifndef HPR_ENGINE_PREFETCH
 #define HPR_ENGINE_PREFETCH 0  // 1: epilogue inputs loaded before the gather rounds
@@ -275,11 +275,23 @@ constexpr int kSumUnroll = HPR_ENGINE_SUM_UNROLL > 0 ? HPR_ENGINE_SUM_UNROLL : 1
 
 constexpr bool kTwoRows = kRowCap > 32;   // a lane owns rows lane and lane + 32
 
+#ifndef HPR_ENGINE_RUNS
+#define HPR_ENGINE_RUNS 1  // 1: run layout, row sums in registers; 0: products staged in shared memory
+#endif
+
+#if HPR_ENGINE_RUNS
+struct WarpSmem {
+  double acc[kRowCap];  // row sums by non-empty ordinal, then raw cone values by row
+  double ns[kRowCap];   // per-cone norms at the cone's first row
+  int32_t aux[kRowCap]; // cone heads
+};
+#else
 struct WarpSmem {
   double prod[kNnzTile];  // products, later per-cone norms
   double acc[kRowCap];    // row sums / raw cone values
   int32_t aux[kRowCap];   // cone heads
 };
+#endif
 
 __device__ __forceinline__ bool tile_is_cone(const Task& t, bool cones) {
   return cones && (t.kind == TASK_CONE_PART || t.cone >= 0);
@@ -351,6 +363,257 @@ __device__ __forceinline__ bool arrive_big(const EngineArgs& a, int slot) {
   return __shfl_sync(0xffffffffu, last, 0) != 0;
 }
 
+// Projection and epilogue of a tile's rows once their sums are known (acc0
+// for row rb + lane, acc1 for row rb + lane + 32), shared by both layouts.
+template <class Epi>
+__device__ __forceinline__ void tile_epilogue(const EngineArgs& a, Epi& epi, int tix, const Task& t, bool cone,
+                                              int nrows, double acc0, double acc1, const Vals<Epi::kSlots>& v0,
+                                              const Vals<Epi::kSlots>& v1, double* ns, WarpSmem& ws, Red& red) {
+  const int lane = threadIdx.x & 31;
+  if (!cone) {
+    if (lane < nrows) epi.linear(t.rb + lane, acc0, v0, red);
+    if (kTwoRows && lane + 32 < nrows) epi.linear(t.rb + lane + 32, acc1, v1, red);
+    if constexpr (Epi::kNRed > 0) {
+      if (t.kind == TASK_CONE_PART && lane == 0) {
+        double* dst = a.red_slots + (int64_t)(a.pv.ntasks + t.group) * kMaxRed;
+        for (int k = 0; k < Epi::kNRed; ++k) dst[k] = 0.0;
+      }
+    }
+  } else if (t.kind == TASK_CONE_PART) {
+    if (lane < nrows) a.pv.raw[t.rb + lane] = epi.cone_raw(t.rb + lane, acc0, v0, red);
+    if (kTwoRows && lane + 32 < nrows) a.pv.raw[t.rb + lane + 32] = epi.cone_raw(t.rb + lane + 32, acc1, v1, red);
+    if (arrive_big(a, t.group)) finalize_big_cone(a, epi, t.group);
+  } else {
+    // whole small cones: raw values in place, one lane per cone for the
+    // norm (ascending order, like the reference), one lane per row for the
+    // projection.
+    if (lane < nrows) ws.acc[lane] = epi.cone_raw(t.rb + lane, acc0, v0, red);
+    if (kTwoRows && lane + 32 < nrows) ws.acc[lane + 32] = epi.cone_raw(t.rb + lane + 32, acc1, v1, red);
+    __syncwarp();
+    for (int k = lane; k < t.ncones; k += 32) {
+      int c0 = __ldg(a.pv.cone_start + t.cone + k) - t.rb;
+      int c1 = __ldg(a.pv.cone_start + t.cone + k + 1) - t.rb;
+      double ss = 0.0;
+      for (int j = c0 + 1; j < c1; ++j) ss += ws.acc[j] * ws.acc[j];
+      ns[c0] = sqrt(ss);
+      for (int j = c0; j < c1; ++j) ws.aux[j] = c0;
+    }
+    __syncwarp();
+    if (lane < nrows) {
+      int h = ws.aux[lane];
+      epi.cone_apply(t.rb + lane, ws.acc[lane], ws.acc[h], ns[h], lane == h, v0, red);
+    }
+    if (kTwoRows && lane + 32 < nrows) {
+      int r = lane + 32, h = ws.aux[r];
+      epi.cone_apply(t.rb + r, ws.acc[r], ws.acc[h], ns[h], r == h, v1, red);
+    }
+  }
+  __syncwarp();
+
+  // ---- per-tile reduction slot
+  if constexpr (Epi::kNRed > 0) {
+    warp_reduce<Epi::kNRed, Epi::kMaxMask>(red);
+    if (lane == 0) {
+      double* dst = a.red_slots + (int64_t)tix * kMaxRed;
+      for (int k = 0; k < Epi::kNRed; ++k) dst[k] = red.v[k];
+    }
+  }
+}
+
+// The last slice of a long row: add the slice partials in slice order and
+// finish the row (and its cone, when the row belongs to a split cone).
+template <class Epi>
+__device__ __forceinline__ void long_row_part(const EngineArgs& a, Epi& epi, int tix, const Task& t, double ps) {
+  const int lane = threadIdx.x & 31;
+  const LongRow lr = a.pv.lng[t.group];
+  int last = 0;
+  if (lane == 0) {
+    a.pv.partials[lr.partial_base + t.part] = ps;
+    __threadfence();
+    int old = atomicAdd(a.pv.lng_cnt + t.group, 1);
+    last = (old == lr.nparts - 1) ? 1 : 0;
+  }
+  if (__shfl_sync(0xffffffffu, last, 0)) {
+    __threadfence();
+    double tot = 0.0;
+    if (lane == 0) {
+      for (int p = 0; p < lr.nparts; ++p) tot = tot + __ldcg(a.pv.partials + lr.partial_base + p);
+      a.pv.lng_cnt[t.group] = 0;
+    }
+    const bool to_cone = Epi::kCones && lr.bigcone >= 0;
+    Red lred;
+    red_init<Epi::kNRed, Epi::kMaxMask>(lred);
+    if (lane == 0) {
+      Vals<Epi::kSlots> v;
+      load_vals<Epi>(v, epi, to_cone, lr.row);
+      if (!to_cone) epi.linear(lr.row, tot, v, lred);
+      else a.pv.raw[lr.row] = epi.cone_raw(lr.row, tot, v, lred);
+      if constexpr (Epi::kNRed > 0) {
+        double* dst = a.red_slots + (int64_t)(a.pv.ntasks + a.pv.nbig + t.group) * kMaxRed;
+        for (int k = 0; k < Epi::kNRed; ++k) dst[k] = lred.v[k];
+      }
+    }
+    if (to_cone && arrive_big(a, lr.bigcone)) finalize_big_cone(a, epi, lr.bigcone);
+  }
+  if constexpr (Epi::kNRed > 0) {
+    // this tile's own slot carries nothing
+    if (lane == 0)
+      for (int k = 0; k < Epi::kNRed; ++k) a.red_slots[(int64_t)tix * kMaxRed + k] = 0.0;
+  }
+}
+
+#if HPR_ENGINE_RUNS
+// One tile in the run layout (TileRun).  Lane L owns run L: R = ceil(nnz/32)
+// consecutive nonzeros of the tile, stored at slots sbase + 32 k + L.  Per
+// step the warp requests U column/value pairs per lane (coalesced, streamed
+// evict-first), the next step's pairs, and then the U gathers of xin; each
+// lane adds its products in column order (a separate multiply and add, as
+// the reference's sequential product), closing a row sum at every row start
+// the lane's descriptor marks.  A row inside one run is thus summed exactly
+// as the reference sums it.  A row that began in an earlier run (the run's
+// first segment) is a continuation: the continuations of one row are added
+// in a fixed-order segmented scan over the lanes and then to the row's head
+// segment.  Row sums are indexed by non-empty ordinal in shared memory and
+// read back by the lanes that own the rows.
+// kCoherent: the gathered vector may have been written earlier in the same
+// launch (the fused multi-iteration kernel), so it is read through L2
+// instead of the read-only path.
+// CH (U): nonzeros per lane per step.
+template <class Epi, int PREC, bool kCoherent = false, int CH = kChunk>
+__device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSmem& ws) {
+  constexpr int U = CH;
+  const int lane = threadIdx.x & 31;
+  const Task t = a.pv.tasks[tix];
+  const TileRun tr = a.pv.runs[tix];
+  const uint32_t desc = a.pv.desc[(int64_t)tix * 32 + lane];
+  const int nrows = t.re - t.rb;
+  const int nnz = t.nze - t.nzb;
+  const int R = (nnz + 31) >> 5;
+  int my = nnz - lane * R;
+  my = my < 0 ? 0 : (my > R ? R : my);
+  const bool cone = tile_is_cone(t, Epi::kCones);
+  const uint64_t pol = HPR_ENGINE_STREAM == 2 ? l2_evict_first_policy() : 0;
+  const uint32_t heads = desc & ((1u << kDescOrdShift) - 1u);
+  const int j0 = (int)(desc >> kDescOrdShift);
+  Vals<Epi::kSlots> v0, v1;
+  if (HPR_ENGINE_PREFETCH && t.kind != TASK_LONG_PART) {
+    if (lane < nrows) load_vals<Epi>(v0, epi, cone, t.rb + lane);
+    if (kTwoRows && lane + 32 < nrows) load_vals<Epi>(v1, epi, cone, t.rb + lane + 32);
+  }
+
+  // ---- 1. products, added per lane in column order
+  const int64_t base = (int64_t)tr.sbase + lane;
+  double s = 0.0, cont = 0.0;
+  int cur = j0 - 1;  // non-empty ordinal of the row being summed
+  {
+    auto load_step = [&](int k0, int32_t* cc, double* vv) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + u;
+        cc[u] = 0;
+        vv[u] = 0.0;
+        if (k < my) {
+          const int64_t e = base + 32 * (int64_t)k;
+          cc[u] = ld_stream(a.pv.tcol + e, pol);
+          if constexpr (PREC == HPR_PREC_FP64) vv[u] = ld_stream(a.pv.tval + e, pol);
+          else if constexpr (PREC == HPR_PREC_FP32) vv[u] = (double)__ldcs(a.pv.tval32 + e);
+          else vv[u] = (double)__uint_as_float(((unsigned int)__ldcs(reinterpret_cast<const unsigned short*>(a.pv.tval16) + e)) << 16);
+        }
+      }
+    };
+    int32_t cols[U];
+    double vals[U];
+    load_step(0, cols, vals);
+    for (int k0 = 0; k0 < R; k0 += U) {
+      int32_t ncols[U];
+      double nvals[U];
+      if (HPR_ENGINE_PIPE && k0 + U < R) load_step(k0 + U, ncols, nvals);
+      double p[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        p[u] = 0.0;
+        if (k0 + u < my) {
+          if constexpr (PREC == HPR_PREC_FP64)
+            p[u] = vals[u] * (kCoherent ? __ldcg(a.xin + cols[u]) : ld_gather(a.xin + cols[u]));
+          else
+            p[u] = (double)((float)vals[u] * (kCoherent ? __ldcg(a.xin32 + cols[u]) : ld_gather(a.xin32 + cols[u])));
+        }
+      }
+      if (!HPR_ENGINE_PIPE && k0 + U < R) load_step(k0 + U, ncols, nvals);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + u;
+        if (k < my) {
+          if ((heads >> k) & 1u) {
+            // a row starts here: close the previous segment
+            if (cur >= j0) ws.acc[cur] = s;
+            else cont = s;
+            ++cur;
+            s = 0.0;
+          }
+          s = s + p[u];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        cols[u] = ncols[u];
+        vals[u] = nvals[u];
+      }
+    }
+  }
+  if (my > 0) {
+    if (cur >= j0) ws.acc[cur] = s;
+    else cont = s;
+  }
+
+  Red red;
+  red_init<Epi::kNRed, Epi::kMaxMask>(red);
+  if (t.kind == TASK_LONG_PART) {
+    // ---- partial sum of one long row: the runs in a fixed-order warp sum
+    long_row_part(a, epi, tix, t, warp_sum_bcast(cont));
+    return;
+  }
+
+  // without the prefetch, the epilogue inputs are requested here, so they
+  // are not live in registers during the gather steps
+  if (!HPR_ENGINE_PREFETCH) {
+    if (lane < nrows) load_vals<Epi>(v0, epi, cone, t.rb + lane);
+    if (kTwoRows && lane + 32 < nrows) load_vals<Epi>(v1, epi, cone, t.rb + lane + 32);
+  }
+
+  // ---- 2. continuations: segmented scan over the lanes, then added to the
+  // row's head segment
+  {
+    const bool has_cont = my > 0 && !(heads & 1u);
+    const int key = has_cont ? j0 - 1 : -2 - lane;
+    double v = has_cont ? cont : 0.0;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const double o = __shfl_up_sync(0xffffffffu, v, d);
+      const int ok = __shfl_up_sync(0xffffffffu, key, d);
+      if (lane >= d && ok == key) v = o + v;
+    }
+    const int nk = __shfl_down_sync(0xffffffffu, key, 1);
+    __syncwarp();  // head segments are in ws.acc
+    if (has_cont && (lane == 31 || nk != key)) ws.acc[key] = ws.acc[key] + v;
+    __syncwarp();
+  }
+
+  // ---- 3. row sums to the owning lanes (empty rows sum to zero)
+  double acc0 = 0.0, acc1 = 0.0;
+  {
+    const unsigned lt = (1u << lane) - 1u;
+    const unsigned b0 = (unsigned)(tr.nonempty & 0xffffffffull);
+    const unsigned b1 = (unsigned)(tr.nonempty >> 32);
+    if ((b0 >> lane) & 1u) acc0 = ws.acc[__popc(b0 & lt)];
+    if (kTwoRows && ((b1 >> lane) & 1u)) acc1 = ws.acc[__popc(b0) + __popc(b1 & lt)];
+    __syncwarp();
+  }
+
+  // ---- 4. epilogue
+  tile_epilogue<Epi>(a, epi, tix, t, cone, nrows, acc0, acc1, v0, v1, ws.ns, ws, red);
+}
+#else
 // kCoherent: the gathered vector may have been written earlier in the same
 // launch (the fused multi-iteration kernel), so it is read through L2
 // instead of the read-only path.
@@ -601,6 +864,8 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
     }
   }
 }
+
+#endif  // HPR_ENGINE_RUNS
 
 constexpr int kEngineSmem = kWarpsPerCta * (int)sizeof(WarpSmem);
 

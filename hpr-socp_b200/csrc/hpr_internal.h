@@ -17,10 +17,11 @@ namespace hpr {
 // ---------------------------------------------------------------------------
 // Tiling of the fused SpMV + epilogue engine.
 //   One warp processes one Task (tile) at a time: at most kNnzTile nonzeros
-//   of at most kRowCap consecutive rows.  The tile's products are formed in
-//   the warp's shared-memory buffer and each row of at most kSerialMax
-//   nonzeros is summed in column order by one lane, so its result is
-//   bit-identical to the reference's sequential CSC/CSR accumulation.
+//   of at most kRowCap consecutive rows.  Each lane adds a contiguous run of
+//   the tile's products in column order in registers (the run layout,
+//   TileRun below); a row that lies inside one run is summed exactly as the
+//   reference's sequential CSC/CSR accumulation, a row that spans runs adds
+//   its run partials in a fixed order.
 //   kThreads is the block size of the plain reduction and map kernels.
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;
@@ -55,6 +56,24 @@ struct Task {
 };
 static_assert(sizeof(Task) == 32, "Task layout");
 
+// The run layout of a tile (HPR_ENGINE_RUNS).  A tile of nnz nonzeros is
+// cut into 32 contiguous runs of R = ceil(nnz / 32) nonzeros, run L for lane
+// L, and stored lane-interleaved: element k of run L sits at slot
+// sbase + 32 k + L of the plan's tiled column/value arrays, so each load of
+// the warp is coalesced while every lane adds its own run in column order.
+// `desc[32 t + L]` holds the row starts inside run L (bit k: a non-empty row
+// begins at run element k) and, from bit kDescOrdShift, the number of
+// non-empty rows that begin in runs 0..L-1.  `nonempty` marks the tile's
+// non-empty rows (bit r for row rb + r).
+struct TileRun {
+  uint64_t nonempty;
+  int32_t sbase;
+  int32_t pad;
+};
+static_assert(sizeof(TileRun) == 16, "TileRun layout");
+constexpr int kDescOrdShift = 25;
+static_assert(kNnzTile <= 32 * kDescOrdShift, "a run's row-start bits must fit below kDescOrdShift");
+
 struct BigCone {
   int32_t cone, rb, re, nparts;
 };
@@ -68,6 +87,9 @@ struct Plan {
   std::vector<BigCone> big;
   std::vector<LongRow> lng;
   int32_t npartials = 0;  // long-row partial sums
+  std::vector<TileRun> runs;   // per tile (run layout)
+  std::vector<uint32_t> desc;  // per tile and lane (run layout)
+  int64_t tslots = 0;          // slots of the tiled arrays (nonzeros + run padding)
   // device copies
   Task* d_tasks = nullptr;
   BigCone* d_big = nullptr;
@@ -77,6 +99,17 @@ struct Plan {
   double* d_partials = nullptr;  // long-row partial sums
   double* d_raw = nullptr;       // big-cone raw values (nrows)
   int32_t* d_ctr = nullptr;      // [0] tile counter, [1] finished warps
+  TileRun* d_runs = nullptr;
+  uint32_t* d_desc = nullptr;
+  // the matrix this plan serves, in the run layout (built by ensure_tiled
+  // from the CSR arrays; rebuilt when the matrix's values change)
+  mutable int32_t* d_tcol = nullptr;
+  mutable double* d_tval = nullptr;
+  mutable float* d_tval32 = nullptr;
+  mutable __nv_bfloat16* d_tval16 = nullptr;
+  mutable const void* tiled_of = nullptr;  // the DevCSR the arrays were built from
+  mutable int64_t tiled_version = -1;      // its value version then
+  mutable int64_t tiled_version32 = -1;    // its reduced-precision version then
   int32_t nslots() const {
     return (int32_t)tasks.size() + (int32_t)big.size() + (int32_t)lng.size();
   }
@@ -88,6 +121,8 @@ struct Plan {
 // `nnz_cap` (<= kNnzTile; 0: kNnzTile) caps the nonzeros of a tile.
 void build_plan(const std::vector<int32_t>& rowptr, int64_t nrows,
                 const std::vector<int64_t>& cone_starts, Plan& plan, int nnz_cap = 0);
+// the run layout of the plan's tiles (called by build_plan)
+void build_runs(const std::vector<int32_t>& rowptr, Plan& plan);
 
 struct DevCSR {
   int64_t nrows = 0, ncols = 0, nnz = 0;
@@ -96,6 +131,8 @@ struct DevCSR {
   double* val = nullptr;
   float* val32 = nullptr;
   __nv_bfloat16* val16 = nullptr;
+  int64_t version = 0;    // bumped whenever val changes (upload, scaling)
+  int64_t version32 = 0;  // bumped whenever val32 / val16 are re-packed
 };
 
 // Scalars read by the kernels; lives in device memory so captured graphs stay
@@ -123,6 +160,13 @@ struct PlanView {
   int32_t* task_ctr;          // next tile to take
   int32_t* done_ctr;          // CTAs that finished (last one resets both)
   int32_t ntasks, nbig, nlng;
+  // run layout
+  const TileRun* runs;
+  const uint32_t* desc;
+  const int32_t* tcol;
+  const double* tval;
+  const float* tval32;
+  const __nv_bfloat16* tval16;
 };
 
 struct Ctx {
@@ -222,6 +266,11 @@ int dev_alloc_n(Ctx* c, T** p, int64_t n) {
 
 // kernel launchers (hpr_kernels.cu)
 int upload_plan(Ctx* c, Plan& p);
+// the plan's tiled copy of M (run layout), rebuilt when M's values changed;
+// refused inside a stream capture (it may allocate)
+int ensure_tiled(Ctx* c, const DevCSR& M, const Plan& p);
+// ensure_tiled for every matrix side of the context
+int prepare_engine(Ctx* c);
 PlanView view_of(const Plan& p, const int32_t* cone_start);
 int launch_iteration(Ctx* c, bool full);
 int run_iterations(Ctx* c, int64_t k, bool full_last);

@@ -480,6 +480,15 @@ int upload_plan(Ctx* c, Plan& p) {
   HPR_TRY(dev_alloc_n(c, &p.d_partials, (int64_t)p.npartials));
   HPR_TRY(dev_alloc_n(c, &p.d_raw, p.nrows));
   HPR_TRY(dev_alloc_n(c, &p.d_ctr, 2));
+  if (p.tslots > INT32_MAX)
+    return set_err(c, HPR_E_UNSUPPORTED, "matrix too large for the engine's int32 tile layout");
+  HPR_TRY(dev_alloc_n(c, &p.d_runs, nt));
+  HPR_TRY(dev_alloc_n(c, &p.d_desc, nt * 32));
+  if (nt) {
+    HPR_CUDA(c, cudaMemcpyAsync(p.d_runs, p.runs.data(), nt * sizeof(TileRun), cudaMemcpyHostToDevice, c->stream));
+    HPR_CUDA(c, cudaMemcpyAsync(p.d_desc, p.desc.data(), nt * 32 * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                c->stream));
+  }
   if (nt)
     HPR_CUDA(c, cudaMemcpyAsync(p.d_tasks, p.tasks.data(), nt * sizeof(Task), cudaMemcpyHostToDevice, c->stream));
   if (!p.big.empty())
@@ -517,7 +526,106 @@ PlanView view_of(const Plan& p, const int32_t* cone_start) {
   v.ntasks = (int32_t)p.tasks.size();
   v.nbig = (int32_t)p.big.size();
   v.nlng = (int32_t)p.lng.size();
+  v.runs = p.d_runs;
+  v.desc = p.d_desc;
+  v.tcol = p.d_tcol;
+  v.tval = p.d_tval;
+  v.tval32 = p.d_tval32;
+  v.tval16 = p.d_tval16;
   return v;
+}
+
+// ---------------------------------------------------------------------------
+// Run layout of a matrix (TileRun): one warp per tile copies the tile's
+// column indices and values from CSR order to lane-interleaved order; the
+// padding slots of the last runs hold column 0 and value 0 (the engine never
+// reads them).
+// ---------------------------------------------------------------------------
+namespace {
+template <class T>
+__global__ void tile_layout_kernel(const Task* __restrict__ tasks, const TileRun* __restrict__ runs, int ntasks,
+                                   const int32_t* __restrict__ col, const T* __restrict__ val,
+                                   int32_t* __restrict__ tcol, T* __restrict__ tval) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t ti = w0; ti < ntasks; ti += nw) {
+    const Task t = tasks[ti];
+    const int32_t nnz = t.nze - t.nzb;
+    const int32_t R = (nnz + 31) / 32;
+    const int64_t sb = runs[ti].sbase;
+    for (int32_t k = 0; k < R; ++k) {
+      const int32_t e = lane * R + k;  // element k of this lane's run
+      const int64_t d = sb + 32 * (int64_t)k + lane;
+      if (e < nnz) {
+        if (tcol) tcol[d] = col[t.nzb + e];
+        tval[d] = val[t.nzb + e];
+      } else {
+        if (tcol) tcol[d] = 0;
+        tval[d] = T(0.0f);
+      }
+    }
+  }
+}
+
+template <class T>
+int tile_layout(Ctx* c, const Plan& p, const int32_t* col, const T* val, int32_t* tcol, T* tval) {
+  const int nt = (int)p.tasks.size();
+  if (nt == 0) return HPR_OK;
+  const int blocks = std::min(148 * 8, (nt + 7) / 8);
+  tile_layout_kernel<T><<<blocks, 256, 0, c->stream>>>(p.d_tasks, p.d_runs, nt, col, val, tcol, tval);
+  c->launches++;
+  HPR_CUDA(c, cudaGetLastError());
+  return HPR_OK;
+}
+}  // namespace
+
+int ensure_tiled(Ctx* c, const DevCSR& M, const Plan& p) {
+  const bool want32 = M.val32 != nullptr || M.val16 != nullptr;
+  const bool ok64 = p.tiled_of == (const void*)&M && p.tiled_version == M.version && p.d_tval;
+  const bool ok32 = !want32 || (p.tiled_of == (const void*)&M && p.tiled_version32 == M.version32 &&
+                                (!M.val32 || p.d_tval32) && (!M.val16 || p.d_tval16));
+  if (ok64 && ok32) return HPR_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  HPR_CUDA(c, cudaStreamIsCapturing(c->stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone)
+    return set_err(c, HPR_E_CUDA, "engine layout must be prepared before a stream capture");
+  const int64_t ns = std::max<int64_t>(p.tslots, 1);
+  if (p.tiled_of != (const void*)&M) {
+    // another matrix of the same plan (Q or F' on planQ): rebuild everything
+    p.tiled_version = p.tiled_version32 = -1;
+    p.tiled_of = &M;
+  }
+  if (!ok64) {
+    if (!p.d_tcol) HPR_TRY(dev_alloc_n(c, &p.d_tcol, ns));
+    if (!p.d_tval) HPR_TRY(dev_alloc_n(c, &p.d_tval, ns));
+    HPR_TRY(tile_layout<double>(c, p, M.col, M.val, p.d_tcol, p.d_tval));
+    p.tiled_version = M.version;
+  }
+  if (want32 && (!ok32 || !ok64)) {
+    if (M.val32) {
+      if (!p.d_tval32) HPR_TRY(dev_alloc_n(c, &p.d_tval32, ns));
+      HPR_TRY(tile_layout<float>(c, p, nullptr, M.val32, nullptr, p.d_tval32));
+    }
+    if (M.val16) {
+      if (!p.d_tval16) HPR_TRY(dev_alloc_n(c, &p.d_tval16, ns));
+      HPR_TRY(tile_layout<__nv_bfloat16>(c, p, nullptr, M.val16, nullptr, p.d_tval16));
+    }
+    p.tiled_version32 = M.version32;
+  }
+  return HPR_OK;
+}
+
+int prepare_engine(Ctx* c) {
+  if (!c->uploaded) return HPR_OK;
+  HPR_TRY(ensure_tiled(c, c->AT, c->planX));
+  HPR_TRY(ensure_tiled(c, c->A, c->planY));
+  if (c->q_kind == HPR_Q_CSR) HPR_TRY(ensure_tiled(c, c->Q, c->planQ));
+  if (c->q_kind == HPR_Q_DIAG_LOWRANK) {
+    HPR_TRY(ensure_tiled(c, c->F, c->planF));
+    HPR_TRY(ensure_tiled(c, c->FT, c->planQ));
+  }
+  return HPR_OK;
 }
 
 namespace {
@@ -583,6 +691,7 @@ int engine_launch(Ctx* c, const DevCSR& M, const Plan& p, const int32_t* cone_st
     }
     return HPR_OK;
   }
+  HPR_TRY(ensure_tiled(c, M, p));
   EngineArgs a;
   a.M = M;
   a.xin = xin;
@@ -921,6 +1030,7 @@ bool fused_eligible(const Ctx* c) {
 
 // k iterations (the last one full when full_last) in one launch.
 int launch_fused(Ctx* c, int64_t k, bool full_last) {
+  HPR_TRY(prepare_engine(c));
   const bool fp32 = c->precision != HPR_PREC_FP64;
   IterEpis P, F;
   make_iter_epis(c, false, P);
@@ -1479,6 +1589,7 @@ __global__ void __launch_bounds__(kEngineThreads, 1)
 }
 
 int power_fused_A(Ctx* c, int maxit, double tol, double* lam) {
+  HPR_TRY(prepare_engine(c));
   std::vector<double> hz(c->m);
   power_start_vector(hz, 1);
   HPR_CUDA(c, cudaMemcpyAsync(c->pz, hz.data(), c->m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -1724,7 +1835,9 @@ int repack_values(Ctx* c) {
       v32[i] = (float)v[i];
       v16[i] = __double2bfloat16(v[i]);
     }));
+    ++M->version32;
   }
+  HPR_TRY(prepare_engine(c));
   // FP32 gather copies of y (vtmp_m) and x_hat (vtmp_n) are kept by the
   // epilogues; seed them from the current iterates.
   if (c->m > 0) {
@@ -1801,6 +1914,9 @@ int engine_launch_into(Ctx* c, const DevCSR& M, const Plan& p, const int32_t* co
     HPR_CUDA(c, cudaMemsetAsync(out, 0, Epi::kNRed * sizeof(double), c->stream));
     return HPR_OK;
   }
+  // the tiled copy was allocated by hpr_upload; refreshing it allocates nothing
+  if (!p.d_tcol || !p.d_tval) return set_err(c, HPR_E_STATE, "engine layout missing (upload incomplete)");
+  HPR_TRY(ensure_tiled(c, M, p));
   EngineArgs a;
   a.M = M;
   a.xin = xin;

