@@ -77,6 +77,10 @@ void free_all(Ctx* c) {
     f(p->d_ctr);
     f(p->d_runs);
     f(p->d_desc);
+    f(p->d_cpart);
+    f(p->d_bignorm);
+    f(p->d_big_ready);
+    f(p->d_apply_cnt);
     f(p->d_tcol);
     f(p->d_tval);
     f(p->d_tval32);

@@ -117,7 +117,8 @@ __device__ void block_reduce(Red& r, double (*s_red)[kThreads / 32]) {
 // Cache operators of the engine's loads (defaults measured best on B200:
 // gathers through L2 only, streams and epilogue inputs evict-first):
 //   gathers of xin:      0 ld.global.nc, 1 ld.global.cg (L2 only),
-//                        2 ld.global.nc.L1::no_allocate;
+//                        2 ld.global.nc.L1::no_allocate, 3 ld.global.cg with
+//                          an L2 evict-last policy;
 //   col / val streams:   0 ld.global.cs, 1 ld.global.cg,
 //                        2 ld.global.nc.L1::no_allocate with an L2 evict-first
 //                          policy, 3 ld.global.nc;
@@ -158,10 +159,26 @@ __device__ __forceinline__ double ld_stream_pol(const double* p, uint64_t pol) {
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
   return v;
 }
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ double ld_cg_last(const double* p) {
+  double v;
+  asm("ld.global.cg.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(l2_evict_last_policy()));
+  return v;
+}
+__device__ __forceinline__ float ld_cg_last(const float* p) {
+  float v;
+  asm("ld.global.cg.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(l2_evict_last_policy()));
+  return v;
+}
 template <class T>
 __device__ __forceinline__ T ld_gather(const T* p) {
   if constexpr (HPR_ENGINE_GATHER == 1) return __ldcg(p);
   else if constexpr (HPR_ENGINE_GATHER == 2) return ld_nc_na(p);
+  else if constexpr (HPR_ENGINE_GATHER == 3) return ld_cg_last(p);
   else return __ldg(p);
 }
 template <class T>
@@ -216,16 +233,6 @@ struct EngineArgs {
   int bump_inner;       // advance st->inner after the launch
 };
 
-// Matrix values in the precision of the SpMV stream.
-template <int PREC>
-__device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
-  if constexpr (PREC == HPR_PREC_FP32) {
-    return __ldcs(M.val32 + e);
-  } else {
-    unsigned short b = __ldcs(reinterpret_cast<const unsigned short*>(M.val16) + e);
-    return __uint_as_float(((unsigned int)b) << 16);
-  }
-}
 
 // Build-time tuning (defaults measured best on B200): warps per CTA, CTAs
 // per SM requested from the register allocator, tiles per atomic grab and
@@ -242,26 +249,18 @@ __device__ __forceinline__ float ldval32(const DevCSR& M, int64_t e) {
 #ifndef HPR_ENGINE_PREFETCH
 #define HPR_ENGINE_PREFETCH 0  // 1: epilogue inputs loaded before the gather rounds
 #endif
+#ifndef HPR_ENGINE_L2PF
+#define HPR_ENGINE_L2PF 0  // 1: a tile's column/value stream and epilogue rows are prefetched to L2 at its start;
+                           // 2: also the next tile's, after the current tile's gathers (with an early grab)
+#endif
 #ifndef HPR_ENGINE_EARLYGRAB
-#define HPR_ENGINE_EARLYGRAB 0
+#define HPR_ENGINE_EARLYGRAB (HPR_ENGINE_L2PF >= 2)
 #endif
 #ifndef HPR_ENGINE_PIPE
 #define HPR_ENGINE_PIPE 1  // next round's col/val requested before this round's gathers
 #endif
-#ifndef HPR_ENGINE_BIGCONE_UNROLL
-#define HPR_ENGINE_BIGCONE_UNROLL 8  // raw values in flight per lane in a split cone's norm
-#endif
-#ifndef HPR_ENGINE_BIGCONE_APPLY
-#define HPR_ENGINE_BIGCONE_APPLY 1  // rows in flight per lane in a split cone's projection
-#endif
-#ifndef HPR_ENGINE_SUM_PAIR
-#define HPR_ENGINE_SUM_PAIR 0  // 1: a lane sums its two rows in one loop
-#endif
 #ifndef HPR_ENGINE_PDL
 #define HPR_ENGINE_PDL 1  // engine kernels use programmatic dependent launch (0: plain launches)
-#endif
-#ifndef HPR_ENGINE_SUM_UNROLL
-#define HPR_ENGINE_SUM_UNROLL 0  // unrolling of the serial row sums (0: the compiler's choice)
 #endif
 
 constexpr int kWarpsPerCta = HPR_ENGINE_WARPS;
@@ -271,83 +270,129 @@ constexpr int kEngineThreads = kWarpsPerCta * 32;
 #endif
 constexpr int kGrab = HPR_ENGINE_GRAB;  // tiles taken per atomic
 constexpr int kChunk = HPR_ENGINE_CHUNK;  // elements per lane per gather round
-constexpr int kSumUnroll = HPR_ENGINE_SUM_UNROLL > 0 ? HPR_ENGINE_SUM_UNROLL : 1;
 
 constexpr bool kTwoRows = kRowCap > 32;   // a lane owns rows lane and lane + 32
 
-#ifndef HPR_ENGINE_RUNS
-#define HPR_ENGINE_RUNS 1  // 1: run layout, row sums in registers; 0: products staged in shared memory
-#endif
+// Asynchronous prefetch of a byte range into L2 (no registers, no wait):
+// the 16-byte-aligned cover of [p, p + bytes).  Every device array is
+// 256-byte aligned with 64 bytes of slack after its end, so the cover stays
+// inside the allocation.
+__device__ __forceinline__ void prefetch_l2(const void* p, int64_t bytes) {
+  if (bytes <= 0) return;
+  const uintptr_t b = reinterpret_cast<uintptr_t>(p) & ~(uintptr_t)15;
+  const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + (uintptr_t)bytes + 15) & ~(uintptr_t)15;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b), "r"((uint32_t)(e - b)) : "memory");
+}
 
-#if HPR_ENGINE_RUNS
 struct WarpSmem {
   double acc[kRowCap];  // row sums by non-empty ordinal, then raw cone values by row
   double ns[kRowCap];   // per-cone norms at the cone's first row
   int32_t aux[kRowCap]; // cone heads
 };
-#else
-struct WarpSmem {
-  double prod[kNnzTile];  // products, later per-cone norms
-  double acc[kRowCap];    // row sums / raw cone values
-  int32_t aux[kRowCap];   // cone heads
-};
-#endif
 
 __device__ __forceinline__ bool tile_is_cone(const Task& t, bool cones) {
   return cones && (t.kind == TASK_CONE_PART || t.cone >= 0);
 }
 
-// Finish a cone that was split over several tiles: ||tail||_2 over the raw
-// values (global), then the per-row projection.  Executed by one warp.
-template <class Epi>
-__device__ void finalize_big_cone(const EngineArgs& a, Epi& epi, int slot) {
+#ifndef HPR_SPIN_LIMIT
+#define HPR_SPIN_LIMIT (1 << 22)  // polls of a big cone's ready flag (~0.5 s) before giving up
+#endif
+
+__device__ __forceinline__ int ld_acquire(const int32_t* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// The last slice of a split cone has arrived: ||tail||_2 from the slices'
+// shares (added in slice order), published for the cone's apply tiles.
+// Executed by one warp.
+inline __device__ void publish_big_norm(const EngineArgs& a, int slot, int nred) {
   const BigCone bc = a.pv.big[slot];
-  const double* raw = a.pv.raw;
   const int lane = threadIdx.x & 31;
   __threadfence();
-  // One warp runs over the whole cone (thousands of rows), so each lane
-  // requests several rows before using them: kU raw values for the norm
-  // (still added in ascending order) and kA rows, each with only the inputs
-  // cone_apply reads, for the projection.
-  constexpr int kU = HPR_ENGINE_BIGCONE_UNROLL;
   double part = 0.0;
-  for (int r = bc.rb + 1 + lane; r < bc.re; r += 32 * kU) {
-    double v[kU];
-#pragma unroll
-    for (int u = 0; u < kU; ++u) v[u] = (r + 32 * u < bc.re) ? __ldcg(raw + r + 32 * u) : 0.0;
-#pragma unroll
-    for (int u = 0; u < kU; ++u)
-      if (r + 32 * u < bc.re) part = part + v[u] * v[u];
+  for (int q = lane; q < bc.nparts; q += 32) part = part + __ldcg(a.pv.cpart + bc.part_base + q);
+  const double ns = sqrt(warp_sum_bcast(part));
+  if (lane == 0) {
+    a.pv.bignorm[slot] = ns;
+    // the cone's own reduction slot carries nothing (the apply tiles and the
+    // slices carry the rows' terms)
+    if (nred > 0)
+      for (int k = 0; k < nred; ++k) a.red_slots[(int64_t)(a.pv.ntasks + slot) * kMaxRed + k] = 0.0;
+    a.pv.big_cnt[slot] = 0;
+    __threadfence();
+    atomicExch(a.pv.big_ready + slot, 1);
   }
-  double ns = sqrt(warp_sum_bcast(part));
-  double t = __ldcg(raw + bc.rb);
+}
+
+// A slice's share of ||tail||^2: the squares of its raw values, the cone's
+// first row excluded, in a fixed order.
+__device__ __forceinline__ void big_norm_share(const EngineArgs& a, int slot, int part, double sq) {
+  const double tot = warp_sum_bcast(sq);
+  if ((threadIdx.x & 31) == 0) a.pv.cpart[a.pv.big[slot].part_base + part] = tot;
+}
+
+// Projection of rows [t.rb, t.re) of a split cone (TASK_CONE_APPLY): waits
+// for the cone's published norm.  Apply tiles are queued after every slice,
+// so the slices were all taken before any apply tile and the wait is short;
+// it gives up after HPR_SPIN_LIMIT polls, raising HPR_E_TIMEOUT in the
+// device error word, and leaves those rows unprojected.
+template <class Epi>
+__device__ void cone_apply_task(const EngineArgs& a, Epi& epi, int tix, const Task& t) {
+  const int lane = threadIdx.x & 31;
+  const int slot = t.group;
+  int ok = 1;
+  if (lane == 0) {
+    int it = 0;
+    while (ld_acquire(a.pv.big_ready + slot) == 0) {
+      if (++it > HPR_SPIN_LIMIT) {
+        ok = 0;
+        break;
+      }
+      __nanosleep(100);
+    }
+  }
+  ok = __shfl_sync(0xffffffffu, ok, 0);
   Red red;
   red_init<Epi::kNRed, Epi::kMaxMask>(red);
-  constexpr int kA = HPR_ENGINE_BIGCONE_APPLY;
-  constexpr int kN = ApplySlots<Epi>::value;
-  for (int r = bc.rb + lane; r < bc.re; r += 32 * kA) {
-    Vals<Epi::kSlots> v[kA];
-    double rv[kA];
-#pragma unroll
-    for (int u = 0; u < kA; ++u) {
-      rv[u] = 0.0;
-      if (r + 32 * u < bc.re) {
-        load_vals<Epi, kN>(v[u], epi, true, r + 32 * u);
-        rv[u] = __ldcg(raw + r + 32 * u);
-      }
+  if (ok) {
+    __threadfence();
+    const BigCone bc = a.pv.big[slot];
+    const double ns = __ldcg(a.pv.bignorm + slot);
+    const double tv = __ldcg(a.pv.raw + bc.rb);
+    constexpr int kN = ApplySlots<Epi>::value;
+    Vals<Epi::kSlots> v0, v1;
+    double rv0 = 0.0, rv1 = 0.0;
+    const int r0 = t.rb + lane, r1 = t.rb + lane + 32;
+    if (r0 < t.re) {
+      load_vals<Epi, kN>(v0, epi, true, r0);
+      rv0 = __ldcg(a.pv.raw + r0);
     }
-#pragma unroll
-    for (int u = 0; u < kA; ++u)
-      if (r + 32 * u < bc.re) epi.cone_apply(r + 32 * u, rv[u], t, ns, r + 32 * u == bc.rb, v[u], red);
+    if (kTwoRows && r1 < t.re) {
+      load_vals<Epi, kN>(v1, epi, true, r1);
+      rv1 = __ldcg(a.pv.raw + r1);
+    }
+    if (r0 < t.re) epi.cone_apply(r0, rv0, tv, ns, r0 == bc.rb, v0, red);
+    if (kTwoRows && r1 < t.re) epi.cone_apply(r1, rv1, tv, ns, r1 == bc.rb, v1, red);
+  } else if (lane == 0) {
+    atomicExch(&a.st->error, HPR_E_TIMEOUT);
   }
   if constexpr (Epi::kNRed > 0) {
     warp_reduce<Epi::kNRed, Epi::kMaxMask>(red);
     if (lane == 0) {
-      double* dst = a.red_slots + (int64_t)(a.pv.ntasks + slot) * kMaxRed;
+      double* dst = a.red_slots + (int64_t)tix * kMaxRed;
       for (int k = 0; k < Epi::kNRed; ++k) dst[k] = red.v[k];
     }
   }
-  if (lane == 0) a.pv.big_cnt[slot] = 0;
+  // the cone's last apply tile re-arms its flags for the next launch
+  if (lane == 0) {
+    const int old = atomicAdd(a.pv.apply_cnt + slot, 1);
+    if (old == a.pv.big[slot].napply - 1) {
+      a.pv.apply_cnt[slot] = 0;
+      a.pv.big_ready[slot] = 0;
+    }
+  }
 }
 
 // Arrival of one slice on a split cone; true (in every lane) for the warp
@@ -380,9 +425,20 @@ __device__ __forceinline__ void tile_epilogue(const EngineArgs& a, Epi& epi, int
       }
     }
   } else if (t.kind == TASK_CONE_PART) {
-    if (lane < nrows) a.pv.raw[t.rb + lane] = epi.cone_raw(t.rb + lane, acc0, v0, red);
-    if (kTwoRows && lane + 32 < nrows) a.pv.raw[t.rb + lane + 32] = epi.cone_raw(t.rb + lane + 32, acc1, v1, red);
-    if (arrive_big(a, t.group)) finalize_big_cone(a, epi, t.group);
+    const int head = a.pv.big[t.group].rb;
+    double sq = 0.0;
+    if (lane < nrows) {
+      const double r = epi.cone_raw(t.rb + lane, acc0, v0, red);
+      a.pv.raw[t.rb + lane] = r;
+      if (t.rb + lane != head) sq = r * r;
+    }
+    if (kTwoRows && lane + 32 < nrows) {
+      const double r = epi.cone_raw(t.rb + lane + 32, acc1, v1, red);
+      a.pv.raw[t.rb + lane + 32] = r;
+      if (t.rb + lane + 32 != head) sq = sq + r * r;
+    }
+    big_norm_share(a, t.group, t.part, sq);
+    if (arrive_big(a, t.group)) publish_big_norm(a, t.group, Epi::kNRed);
   } else {
     // whole small cones: raw values in place, one lane per cone for the
     // norm (ascending order, like the reference), one lane per row for the
@@ -446,14 +502,21 @@ __device__ __forceinline__ void long_row_part(const EngineArgs& a, Epi& epi, int
     if (lane == 0) {
       Vals<Epi::kSlots> v;
       load_vals<Epi>(v, epi, to_cone, lr.row);
-      if (!to_cone) epi.linear(lr.row, tot, v, lred);
-      else a.pv.raw[lr.row] = epi.cone_raw(lr.row, tot, v, lred);
+      if (!to_cone) {
+        epi.linear(lr.row, tot, v, lred);
+      } else {
+        const double r = epi.cone_raw(lr.row, tot, v, lred);
+        a.pv.raw[lr.row] = r;
+        // the row's share of its cone's ||tail||^2
+        const BigCone bc = a.pv.big[lr.bigcone];
+        a.pv.cpart[bc.part_base + lr.cpart] = lr.row == bc.rb ? 0.0 : r * r;
+      }
       if constexpr (Epi::kNRed > 0) {
         double* dst = a.red_slots + (int64_t)(a.pv.ntasks + a.pv.nbig + t.group) * kMaxRed;
         for (int k = 0; k < Epi::kNRed; ++k) dst[k] = lred.v[k];
       }
     }
-    if (to_cone && arrive_big(a, lr.bigcone)) finalize_big_cone(a, epi, lr.bigcone);
+    if (to_cone && arrive_big(a, lr.bigcone)) publish_big_norm(a, lr.bigcone, Epi::kNRed);
   }
   if constexpr (Epi::kNRed > 0) {
     // this tile's own slot carries nothing
@@ -462,7 +525,34 @@ __device__ __forceinline__ void long_row_part(const EngineArgs& a, Epi& epi, int
   }
 }
 
-#if HPR_ENGINE_RUNS
+// L2 prefetch of tile `tix`: its column and value slots (lanes 0, 1) and
+// its rows of each epilogue input (lanes 2..), so that the tile's loads after
+// the first ones meet L2 instead of DRAM latency.
+template <class Epi, int PREC>
+__device__ __forceinline__ void prefetch_tile(const EngineArgs& a, const Epi& epi, int tix) {
+  const int lane = threadIdx.x & 31;
+  if (lane >= 2 + Epi::kSlots) return;
+  const Task t = a.pv.tasks[tix];
+  if (t.kind == TASK_CONE_APPLY) return;
+  if (lane < 2) {
+    const int64_t sb = a.pv.runs[tix].sbase;
+    const int64_t slots = 32 * (int64_t)((t.nze - t.nzb + 31) >> 5);
+    if (lane == 0) prefetch_l2(a.pv.tcol + sb, slots * 4);
+    else if constexpr (PREC == HPR_PREC_FP64) prefetch_l2(a.pv.tval + sb, slots * 8);
+    else if constexpr (PREC == HPR_PREC_FP32) prefetch_l2(a.pv.tval32 + sb, slots * 4);
+    else prefetch_l2(a.pv.tval16 + sb, slots * 2);
+    return;
+  }
+  if (t.kind == TASK_LONG_PART) return;
+  // (compile-time slot indices keep the epilogue out of local memory)
+  const bool cone = tile_is_cone(t, Epi::kCones);
+  const double* src = nullptr;
+#pragma unroll
+  for (int k = 0; k < Epi::kSlots; ++k)
+    if (lane == 2 + k) src = cone ? epi.cone_src[k] : epi.lin_src[k];
+  if (src) prefetch_l2(src + t.rb, (int64_t)(t.re - t.rb) * 8);
+}
+
 // One tile in the run layout (TileRun).  Lane L owns run L: R = ceil(nnz/32)
 // consecutive nonzeros of the tile, stored at slots sbase + 32 k + L.  Per
 // step the warp requests U column/value pairs per lane (coalesced, streamed
@@ -479,45 +569,67 @@ __device__ __forceinline__ void long_row_part(const EngineArgs& a, Epi& epi, int
 // launch (the fused multi-iteration kernel), so it is read through L2
 // instead of the read-only path.
 // CH (U): nonzeros per lane per step.
+// pf_next >= 0: the warp's next tile, prefetched to L2 after this tile's
+// gathers.
 template <class Epi, int PREC, bool kCoherent = false, int CH = kChunk>
-__device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSmem& ws) {
+__device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSmem& ws, int pf_next = -1) {
   constexpr int U = CH;
   const int lane = threadIdx.x & 31;
-  const Task t = a.pv.tasks[tix];
-  const TileRun tr = a.pv.runs[tix];
+  const Task* tp = a.pv.tasks + tix;
+  if (HPR_ENGINE_L2PF >= 1 && !kCoherent) prefetch_tile<Epi, PREC>(a, epi, tix);
+  if (tp->kind == TASK_CONE_APPLY) {
+    if constexpr (Epi::kCones) {
+      cone_apply_task(a, epi, tix, *tp);
+    } else if constexpr (Epi::kNRed > 0) {
+      // an epilogue without cones treats cone rows as linear rows: nothing
+      // is left to project
+      if (lane == 0)
+        for (int k = 0; k < Epi::kNRed; ++k) a.red_slots[(int64_t)tix * kMaxRed + k] = 0.0;
+    }
+    return;
+  }
+  // only the nonzero range is live during the gathers; the rest of the tile
+  // descriptor is read again afterwards (an L1 hit), which keeps registers
+  // for nonzeros in flight
+  const int nnz = tp->nze - tp->nzb;
   const uint32_t desc = a.pv.desc[(int64_t)tix * 32 + lane];
-  const int nrows = t.re - t.rb;
-  const int nnz = t.nze - t.nzb;
   const int R = (nnz + 31) >> 5;
   int my = nnz - lane * R;
   my = my < 0 ? 0 : (my > R ? R : my);
-  const bool cone = tile_is_cone(t, Epi::kCones);
   const uint64_t pol = HPR_ENGINE_STREAM == 2 ? l2_evict_first_policy() : 0;
   const uint32_t heads = desc & ((1u << kDescOrdShift) - 1u);
   const int j0 = (int)(desc >> kDescOrdShift);
   Vals<Epi::kSlots> v0, v1;
-  if (HPR_ENGINE_PREFETCH && t.kind != TASK_LONG_PART) {
+  if (HPR_ENGINE_PREFETCH && tp->kind != TASK_LONG_PART) {
+    const Task t = *tp;
+    const bool cone = tile_is_cone(t, Epi::kCones);
+    const int nrows = t.re - t.rb;
     if (lane < nrows) load_vals<Epi>(v0, epi, cone, t.rb + lane);
     if (kTwoRows && lane + 32 < nrows) load_vals<Epi>(v1, epi, cone, t.rb + lane + 32);
   }
 
   // ---- 1. products, added per lane in column order
-  const int64_t base = (int64_t)tr.sbase + lane;
+  const int64_t base = (int64_t)a.pv.runs[tix].sbase + lane;
   double s = 0.0, cont = 0.0;
   int cur = j0 - 1;  // non-empty ordinal of the row being summed
   {
+    // one base address per array and step; the U loads of a step sit at
+    // fixed offsets from it
     auto load_step = [&](int k0, int32_t* cc, double* vv) {
+      const int64_t e0 = base + 32 * (int64_t)k0;
+      const int32_t* pc = a.pv.tcol + e0;
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int k = k0 + u;
         cc[u] = 0;
         vv[u] = 0.0;
         if (k < my) {
-          const int64_t e = base + 32 * (int64_t)k;
-          cc[u] = ld_stream(a.pv.tcol + e, pol);
-          if constexpr (PREC == HPR_PREC_FP64) vv[u] = ld_stream(a.pv.tval + e, pol);
-          else if constexpr (PREC == HPR_PREC_FP32) vv[u] = (double)__ldcs(a.pv.tval32 + e);
-          else vv[u] = (double)__uint_as_float(((unsigned int)__ldcs(reinterpret_cast<const unsigned short*>(a.pv.tval16) + e)) << 16);
+          cc[u] = ld_stream(pc + 32 * u, pol);
+          if constexpr (PREC == HPR_PREC_FP64) vv[u] = ld_stream(a.pv.tval + e0 + 32 * u, pol);
+          else if constexpr (PREC == HPR_PREC_FP32) vv[u] = (double)__ldcs(a.pv.tval32 + e0 + 32 * u);
+          else
+            vv[u] = (double)__uint_as_float(
+                ((unsigned int)__ldcs(reinterpret_cast<const unsigned short*>(a.pv.tval16) + e0 + 32 * u)) << 16);
         }
       }
     };
@@ -566,6 +678,10 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
     else cont = s;
   }
 
+  if (HPR_ENGINE_L2PF >= 2 && pf_next >= 0) prefetch_tile<Epi, PREC>(a, epi, pf_next);
+  const Task t = *tp;
+  const int nrows = t.re - t.rb;
+  const bool cone = tile_is_cone(t, Epi::kCones);
   Red red;
   red_init<Epi::kNRed, Epi::kMaxMask>(red);
   if (t.kind == TASK_LONG_PART) {
@@ -603,8 +719,9 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
   double acc0 = 0.0, acc1 = 0.0;
   {
     const unsigned lt = (1u << lane) - 1u;
-    const unsigned b0 = (unsigned)(tr.nonempty & 0xffffffffull);
-    const unsigned b1 = (unsigned)(tr.nonempty >> 32);
+    const uint64_t ne = a.pv.runs[tix].nonempty;
+    const unsigned b0 = (unsigned)(ne & 0xffffffffull);
+    const unsigned b1 = (unsigned)(ne >> 32);
     if ((b0 >> lane) & 1u) acc0 = ws.acc[__popc(b0 & lt)];
     if (kTwoRows && ((b1 >> lane) & 1u)) acc1 = ws.acc[__popc(b0) + __popc(b1 & lt)];
     __syncwarp();
@@ -613,259 +730,6 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
   // ---- 4. epilogue
   tile_epilogue<Epi>(a, epi, tix, t, cone, nrows, acc0, acc1, v0, v1, ws.ns, ws, red);
 }
-#else
-// kCoherent: the gathered vector may have been written earlier in the same
-// launch (the fused multi-iteration kernel), so it is read through L2
-// instead of the read-only path.
-// CH: nonzeros per lane per gather round (the multi-CTA engine uses kChunk;
-// the single-CTA kernels, with few warps in flight, load a whole tile per
-// round).
-template <class Epi, int PREC, bool kCoherent = false, int CH = kChunk>
-__device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSmem& ws) {
-  constexpr int kChunk = CH;
-  const int lane = threadIdx.x & 31;
-  const Task t = a.pv.tasks[tix];
-  const int nrows = t.re - t.rb;
-  const int nnz = t.nze - t.nzb;
-  const bool cone = tile_is_cone(t, Epi::kCones);
-  const uint64_t pol = HPR_ENGINE_STREAM == 2 ? l2_evict_first_policy() : 0;
-
-  // ---- 0. row pointers and epilogue inputs of this lane's two rows
-  int r0b = 0, r0e = 0, r1b = 0, r1e = 0;
-  Vals<Epi::kSlots> v0, v1;
-  if (t.kind != TASK_LONG_PART) {
-    if (lane < nrows) {
-      r0b = __ldg(a.M.rowptr + t.rb + lane) - t.nzb;
-      r0e = __ldg(a.M.rowptr + t.rb + lane + 1) - t.nzb;
-      if (HPR_ENGINE_PREFETCH) load_vals<Epi>(v0, epi, cone, t.rb + lane);
-    }
-    if (kTwoRows && lane + 32 < nrows) {
-      r1b = __ldg(a.M.rowptr + t.rb + lane + 32) - t.nzb;
-      r1e = __ldg(a.M.rowptr + t.rb + lane + 33) - t.nzb;
-      if (HPR_ENGINE_PREFETCH) load_vals<Epi>(v1, epi, cone, t.rb + lane + 32);
-    }
-  }
-
-  // ---- 1. products into warp-private shared memory.  The column indices and
-  // values of the next round are requested before the current round's
-  // gathers, so the DRAM stream and the L2 gathers overlap.
-  {
-    auto load_round = [&](int c0, int32_t* cc, double* vv) {
-#pragma unroll
-      for (int k = 0; k < kChunk; ++k) {
-        const int e = c0 + lane + 32 * k;
-        cc[k] = 0;
-        vv[k] = 0.0;
-        if (e < nnz) {
-          cc[k] = ld_stream(a.M.col + t.nzb + e, pol);
-          if constexpr (PREC == HPR_PREC_FP64) vv[k] = ld_stream(a.M.val + t.nzb + e, pol);
-          else vv[k] = (double)ldval32<PREC>(a.M, (int64_t)t.nzb + e);
-        }
-      }
-    };
-    int32_t cols[kChunk];
-    double vals[kChunk];
-    load_round(0, cols, vals);
-    for (int c0 = 0; c0 < nnz; c0 += 32 * kChunk) {
-      int32_t ncols[kChunk];
-      double nvals[kChunk];
-      if (HPR_ENGINE_PIPE && c0 + 32 * kChunk < nnz) load_round(c0 + 32 * kChunk, ncols, nvals);
-#pragma unroll
-      for (int k = 0; k < kChunk; ++k) {
-        const int e = c0 + lane + 32 * k;
-        if (e < nnz) {
-          if constexpr (PREC == HPR_PREC_FP64)
-            ws.prod[e] = vals[k] * (kCoherent ? __ldcg(a.xin + cols[k]) : ld_gather(a.xin + cols[k]));
-          else
-            ws.prod[e] =
-                (double)((float)vals[k] * (kCoherent ? __ldcg(a.xin32 + cols[k]) : ld_gather(a.xin32 + cols[k])));
-        }
-      }
-      if (!HPR_ENGINE_PIPE && c0 + 32 * kChunk < nnz) load_round(c0 + 32 * kChunk, ncols, nvals);
-#pragma unroll
-      for (int k = 0; k < kChunk; ++k) {
-        cols[k] = ncols[k];
-        vals[k] = nvals[k];
-      }
-    }
-  }
-  __syncwarp();
-
-  Red red;
-  red_init<Epi::kNRed, Epi::kMaxMask>(red);
-  if (t.kind == TASK_LONG_PART) {
-    // ---- partial sum of one long row
-    double part = 0.0;
-    for (int e = lane; e < nnz; e += 32) part = part + ws.prod[e];
-    double ps = warp_sum_bcast(part);
-    const LongRow lr = a.pv.lng[t.group];
-    int last = 0;
-    if (lane == 0) {
-      a.pv.partials[lr.partial_base + t.part] = ps;
-      __threadfence();
-      int old = atomicAdd(a.pv.lng_cnt + t.group, 1);
-      last = (old == lr.nparts - 1) ? 1 : 0;
-    }
-    if (__shfl_sync(0xffffffffu, last, 0)) {
-      __threadfence();
-      double tot = 0.0;
-      if (lane == 0) {
-        for (int p = 0; p < lr.nparts; ++p) tot = tot + __ldcg(a.pv.partials + lr.partial_base + p);
-        a.pv.lng_cnt[t.group] = 0;
-      }
-      const bool to_cone = Epi::kCones && lr.bigcone >= 0;
-      Red lred;
-      red_init<Epi::kNRed, Epi::kMaxMask>(lred);
-      if (lane == 0) {
-        Vals<Epi::kSlots> v;
-        load_vals<Epi>(v, epi, to_cone, lr.row);
-        if (!to_cone) epi.linear(lr.row, tot, v, lred);
-        else a.pv.raw[lr.row] = epi.cone_raw(lr.row, tot, v, lred);
-        if constexpr (Epi::kNRed > 0) {
-          double* dst = a.red_slots + (int64_t)(a.pv.ntasks + a.pv.nbig + t.group) * kMaxRed;
-          for (int k = 0; k < Epi::kNRed; ++k) dst[k] = lred.v[k];
-        }
-      }
-      if (to_cone && arrive_big(a, lr.bigcone)) finalize_big_cone(a, epi, lr.bigcone);
-    }
-    if constexpr (Epi::kNRed > 0) {
-      // this tile's own slot carries nothing
-      if (lane == 0)
-        for (int k = 0; k < Epi::kNRed; ++k) a.red_slots[(int64_t)tix * kMaxRed + k] = 0.0;
-    }
-    return;
-  }
-
-  // without the prefetch, the epilogue inputs are requested here, so they
-  // are not live in registers during the gather rounds
-  if (!HPR_ENGINE_PREFETCH) {
-    if (lane < nrows) load_vals<Epi>(v0, epi, cone, t.rb + lane);
-    if (kTwoRows && lane + 32 < nrows) load_vals<Epi>(v1, epi, cone, t.rb + lane + 32);
-  }
-  // ---- 2. row sums
-  bool long0 = false, long1 = false;
-#if HPR_ENGINE_SUM_PAIR
-  if (kTwoRows) {
-    // the lane's two rows summed in one loop: two independent chains, each
-    // in ascending column order
-    const bool s0 = lane < nrows && r0e - r0b <= kSerialMax;
-    const bool s1 = lane + 32 < nrows && r1e - r1b <= kSerialMax;
-    long0 = lane < nrows && !s0;
-    long1 = lane + 32 < nrows && !s1;
-    const int n0 = s0 ? r0e - r0b : 0, n1 = s1 ? r1e - r1b : 0;
-    const int nmax = n0 > n1 ? n0 : n1;
-    double a0 = 0.0, a1 = 0.0;
-    for (int k = 0; k < nmax; ++k) {
-      if (k < n0) a0 = a0 + ws.prod[r0b + k];
-      if (k < n1) a1 = a1 + ws.prod[r1b + k];
-    }
-    if (s0) ws.acc[lane] = a0;
-    if (s1) ws.acc[lane + 32] = a1;
-  } else
-#endif
-  {
-  if (lane < nrows) {
-    if (r0e - r0b <= kSerialMax) {
-      double s = 0.0;
-#if HPR_ENGINE_SUM_UNROLL > 0
-#pragma unroll kSumUnroll
-#endif
-      for (int k = r0b; k < r0e; ++k) s = s + ws.prod[k];
-      ws.acc[lane] = s;
-    } else {
-      long0 = true;
-    }
-  }
-  if (kTwoRows && lane + 32 < nrows) {
-    if (r1e - r1b <= kSerialMax) {
-      double s = 0.0;
-#if HPR_ENGINE_SUM_UNROLL > 0
-#pragma unroll kSumUnroll
-#endif
-      for (int k = r1b; k < r1e; ++k) s = s + ws.prod[k];
-      ws.acc[lane + 32] = s;
-    } else {
-      long1 = true;
-    }
-  }
-  }
-  {
-    unsigned m0 = __ballot_sync(0xffffffffu, long0), m1 = kTwoRows ? __ballot_sync(0xffffffffu, long1) : 0u;
-    while (m0 | m1) {
-      int src_lane, rr;
-      if (m0) {
-        src_lane = __ffs(m0) - 1;
-        m0 &= m0 - 1;
-        rr = src_lane;
-      } else {
-        src_lane = __ffs(m1) - 1;
-        m1 &= m1 - 1;
-        rr = src_lane + 32;
-      }
-      int b0 = __shfl_sync(0xffffffffu, rr < 32 ? r0b : r1b, src_lane);
-      int b1 = __shfl_sync(0xffffffffu, rr < 32 ? r0e : r1e, src_lane);
-      double s = 0.0;
-      for (int k = b0 + lane; k < b1; k += 32) s = s + ws.prod[k];
-      s = warp_sum_bcast(s);
-      if (lane == 0) ws.acc[rr] = s;
-    }
-  }
-  __syncwarp();
-
-  // ---- 3. epilogue
-  if (!cone) {
-    if (lane < nrows) epi.linear(t.rb + lane, ws.acc[lane], v0, red);
-    if (kTwoRows && lane + 32 < nrows) epi.linear(t.rb + lane + 32, ws.acc[lane + 32], v1, red);
-    if constexpr (Epi::kNRed > 0) {
-      if (t.kind == TASK_CONE_PART && lane == 0) {
-        double* dst = a.red_slots + (int64_t)(a.pv.ntasks + t.group) * kMaxRed;
-        for (int k = 0; k < Epi::kNRed; ++k) dst[k] = 0.0;
-      }
-    }
-  } else if (t.kind == TASK_CONE_PART) {
-    if (lane < nrows) a.pv.raw[t.rb + lane] = epi.cone_raw(t.rb + lane, ws.acc[lane], v0, red);
-    if (kTwoRows && lane + 32 < nrows)
-      a.pv.raw[t.rb + lane + 32] = epi.cone_raw(t.rb + lane + 32, ws.acc[lane + 32], v1, red);
-    if (arrive_big(a, t.group)) finalize_big_cone(a, epi, t.group);
-  } else {
-    // whole small cones: raw values in place, one lane per cone for the
-    // norm (ascending order, like the reference), one lane per row for the
-    // projection.
-    if (lane < nrows) ws.acc[lane] = epi.cone_raw(t.rb + lane, ws.acc[lane], v0, red);
-    if (kTwoRows && lane + 32 < nrows) ws.acc[lane + 32] = epi.cone_raw(t.rb + lane + 32, ws.acc[lane + 32], v1, red);
-    __syncwarp();
-    double* ns = ws.prod;  // products are dead
-    for (int k = lane; k < t.ncones; k += 32) {
-      int c0 = __ldg(a.pv.cone_start + t.cone + k) - t.rb;
-      int c1 = __ldg(a.pv.cone_start + t.cone + k + 1) - t.rb;
-      double ss = 0.0;
-      for (int j = c0 + 1; j < c1; ++j) ss += ws.acc[j] * ws.acc[j];
-      ns[c0] = sqrt(ss);
-      for (int j = c0; j < c1; ++j) ws.aux[j] = c0;
-    }
-    __syncwarp();
-    if (lane < nrows) {
-      int h = ws.aux[lane];
-      epi.cone_apply(t.rb + lane, ws.acc[lane], ws.acc[h], ns[h], lane == h, v0, red);
-    }
-    if (kTwoRows && lane + 32 < nrows) {
-      int r = lane + 32, h = ws.aux[r];
-      epi.cone_apply(t.rb + r, ws.acc[r], ws.acc[h], ns[h], r == h, v1, red);
-    }
-  }
-  __syncwarp();
-
-  // ---- 4. per-tile reduction slot
-  if constexpr (Epi::kNRed > 0) {
-    warp_reduce<Epi::kNRed, Epi::kMaxMask>(red);
-    if (lane == 0) {
-      double* dst = a.red_slots + (int64_t)tix * kMaxRed;
-      for (int k = 0; k < Epi::kNRed; ++k) dst[k] = red.v[k];
-    }
-  }
-}
-
-#endif  // HPR_ENGINE_RUNS
 
 constexpr int kEngineSmem = kWarpsPerCta * (int)sizeof(WarpSmem);
 
@@ -912,8 +776,14 @@ __global__ void __launch_bounds__(kEngineThreads, EngineMinBlocks<Epi>::value) e
     // processed, so its atomic latency is hidden behind the tiles
     int next = 0;
     if (HPR_ENGINE_EARLYGRAB && lane == 0) next = atomicAdd(a.pv.task_ctr, kGrab);
-    for (int q = 0; q < kGrab && base + q < ntasks; ++q)
-      process_warp_tile<Epi, PREC, false, EngineChunk<Epi>::value>(a, epi, base + q, ws);
+    for (int q = 0; q < kGrab && base + q < ntasks; ++q) {
+      int pf = -1;
+      if (HPR_ENGINE_L2PF >= 2 && HPR_ENGINE_EARLYGRAB && q == kGrab - 1) {
+        pf = __shfl_sync(0xffffffffu, next, 0);
+        pf = pf < ntasks ? pf : -1;
+      }
+      process_warp_tile<Epi, PREC, false, EngineChunk<Epi>::value>(a, epi, base + q, ws, pf);
+    }
     if (!HPR_ENGINE_EARLYGRAB && lane == 0) next = atomicAdd(a.pv.task_ctr, kGrab);
     base = __shfl_sync(0xffffffffu, next, 0);
   }

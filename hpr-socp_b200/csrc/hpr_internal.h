@@ -35,28 +35,28 @@ constexpr int kNnzTile = HPR_NNZ_TILE;
 #endif
 constexpr int kRowCap = HPR_ENGINE_ROWCAP;  // 32 (one row per lane) or 64 (two)
 static_assert(kRowCap == 32 || kRowCap == 64, "one or two rows per lane");
-constexpr int kSerialMax = 64;      // rows longer than this use a warp reduction
 constexpr int kSmallConeMax = kRowCap;  // larger cones are split over several tiles
 constexpr int kMaxRed = 8;          // reduction lanes per engine launch
 
 enum TaskKind : int16_t {
-  TASK_ROWS = 0,       // complete rows [rb,re); whole cones when cone >= 0
-  TASK_CONE_PART = 1,  // complete rows inside one big cone
-  TASK_LONG_PART = 2,  // a nonzero sub-range of one long row
+  TASK_ROWS = 0,        // complete rows [rb,re); whole cones when cone >= 0
+  TASK_CONE_PART = 1,   // complete rows inside one big cone
+  TASK_LONG_PART = 2,   // a nonzero sub-range of one long row
+  TASK_CONE_APPLY = 3,  // projection of rows [rb,re) of a big cone, once its norm is known
 };
 
 struct Task {
   int32_t rb, re;    // rows
-  int32_t nzb, nze;  // nonzero range
+  int32_t nzb, nze;  // nonzero range (empty for TASK_CONE_APPLY)
   int16_t kind;
   int16_t ncones;    // TASK_ROWS: number of whole cones in the task
-  int32_t cone;      // first cone (TASK_ROWS), the cone (CONE_PART), or -1
-  int32_t group;     // big-cone slot (CONE_PART) / long-row slot (LONG_PART)
-  int32_t part;      // part index within the long row (LONG_PART)
+  int32_t cone;      // first cone (TASK_ROWS), the cone (CONE_PART, CONE_APPLY), or -1
+  int32_t group;     // big-cone slot (CONE_PART, CONE_APPLY) / long-row slot (LONG_PART)
+  int32_t part;      // slice index within the long row (LONG_PART) or the big cone (CONE_PART)
 };
 static_assert(sizeof(Task) == 32, "Task layout");
 
-// The run layout of a tile (HPR_ENGINE_RUNS).  A tile of nnz nonzeros is
+// The run layout of a tile.  A tile of nnz nonzeros is
 // cut into 32 contiguous runs of R = ceil(nnz / 32) nonzeros, run L for lane
 // L, and stored lane-interleaved: element k of run L sits at slot
 // sbase + 32 k + L of the plan's tiled column/value arrays, so each load of
@@ -74,11 +74,19 @@ static_assert(sizeof(TileRun) == 16, "TileRun layout");
 constexpr int kDescOrdShift = 25;
 static_assert(kNnzTile <= 32 * kDescOrdShift, "a run's row-start bits must fit below kDescOrdShift");
 
+// A cone of more than kSmallConeMax rows (or nonzeros beyond one tile) is
+// split: its nparts slices (CONE_PART tiles and long rows) write the raw
+// values and their share of ||tail||^2 (slot part_base + slice); the slice
+// that arrives last adds the shares in slice order and publishes the norm;
+// the cone's napply TASK_CONE_APPLY tiles, queued after every other tile,
+// then project its rows in parallel.
 struct BigCone {
   int32_t cone, rb, re, nparts;
+  int32_t part_base, napply, pad0, pad1;
 };
 struct LongRow {
   int32_t row, nparts, partial_base, bigcone;  // bigcone slot or -1
+  int32_t cpart;                               // slice index within the big cone
 };
 
 struct Plan {
@@ -87,6 +95,7 @@ struct Plan {
   std::vector<BigCone> big;
   std::vector<LongRow> lng;
   int32_t npartials = 0;  // long-row partial sums
+  int32_t ncparts = 0;    // big-cone slices (norm shares)
   std::vector<TileRun> runs;   // per tile (run layout)
   std::vector<uint32_t> desc;  // per tile and lane (run layout)
   int64_t tslots = 0;          // slots of the tiled arrays (nonzeros + run padding)
@@ -101,6 +110,10 @@ struct Plan {
   int32_t* d_ctr = nullptr;      // [0] tile counter, [1] finished warps
   TileRun* d_runs = nullptr;
   uint32_t* d_desc = nullptr;
+  double* d_cpart = nullptr;      // big-cone norm shares per slice
+  double* d_bignorm = nullptr;    // published norm per big cone
+  int32_t* d_big_ready = nullptr; // 1 once the norm is published (reset by the last apply tile)
+  int32_t* d_apply_cnt = nullptr; // apply tiles done per big cone
   // the matrix this plan serves, in the run layout (built by ensure_tiled
   // from the CSR arrays; rebuilt when the matrix's values change)
   mutable int32_t* d_tcol = nullptr;
@@ -159,6 +172,10 @@ struct PlanView {
   const int32_t* cone_start;  // cone start rows (+ sentinel), this side
   int32_t* task_ctr;          // next tile to take
   int32_t* done_ctr;          // CTAs that finished (last one resets both)
+  double* cpart;
+  double* bignorm;
+  int32_t* big_ready;
+  int32_t* apply_cnt;
   int32_t ntasks, nbig, nlng;
   // run layout
   const TileRun* runs;

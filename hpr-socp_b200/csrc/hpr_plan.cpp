@@ -7,8 +7,10 @@
 // rows, so one launch handles linear rows and cones of every size:
 //   * TASK_ROWS       — consecutive linear rows, or consecutive whole cones of
 //                       at most kSmallConeMax rows, finished inside the CTA;
-//   * TASK_CONE_PART  — a slice of a larger cone; the CTA that completes the
-//                       last slice projects the whole cone;
+//   * TASK_CONE_PART  — a slice of a larger cone; the warp that completes
+//                       the last slice publishes the cone's norm;
+//   * TASK_CONE_APPLY — the projection of 64 rows of a larger cone, queued
+//                       after all other tiles;
 //   * TASK_LONG_PART  — a nonzero slice of a row longer than one tile; the CTA
 //                       that completes the last slice adds the partial sums in
 //                       slice order and finishes the row.
@@ -180,15 +182,31 @@ void build_plan(const std::vector<int32_t>& rp, int64_t nrows,
 #endif
   plan.tasks = multi;
   plan.tasks.insert(plan.tasks.end(), rows.begin(), rows.end());
-  // flag tiles holding rows that need the warp-reduction phase
-  for (Task& t : plan.tasks) {
-    if (t.kind == TASK_LONG_PART) continue;
-    t.part = 0;
-    for (int32_t q = t.rb; q < t.re; ++q)
-      if (rp[q + 1] - rp[q] > kSerialMax) {
-        t.part = 1;
-        break;
-      }
+  // big cones: slice numbers, norm-share slots and the apply tiles, which
+  // go last (a warp that takes one finds every slice of every cone taken)
+  std::vector<int32_t> next_part(plan.big.size(), 0);
+  for (Task& t : plan.tasks)
+    if (t.kind == TASK_CONE_PART) t.part = next_part[t.group]++;
+  for (LongRow& lr : plan.lng)
+    if (lr.bigcone >= 0) lr.cpart = next_part[lr.bigcone]++;
+    else lr.cpart = -1;
+  plan.ncparts = 0;
+  for (size_t b = 0; b < plan.big.size(); ++b) {
+    BigCone& bc = plan.big[b];
+    bc.part_base = plan.ncparts;
+    plan.ncparts += bc.nparts;
+    bc.napply = 0;
+    for (int32_t r = bc.rb; r < bc.re; r += kRowCap) {
+      Task t{};
+      t.rb = r;
+      t.re = std::min(bc.re, r + kRowCap);
+      t.nzb = t.nze = rp[r];
+      t.kind = TASK_CONE_APPLY;
+      t.cone = bc.cone;
+      t.group = (int32_t)b;
+      plan.tasks.push_back(t);
+      bc.napply++;
+    }
   }
   build_runs(rp, plan);
 }
@@ -211,6 +229,7 @@ void build_runs(const std::vector<int32_t>& rp, Plan& plan) {
       tr.nonempty = 1;  // one row; its runs carry no row starts
       continue;
     }
+    if (t.kind == TASK_CONE_APPLY) continue;  // no nonzeros
     uint32_t heads[32] = {0};
     for (int32_t q = t.rb; q < t.re; ++q) {
       if (rp[q + 1] <= rp[q]) continue;

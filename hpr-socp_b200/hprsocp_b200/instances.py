@@ -171,6 +171,35 @@ def config2(seed: int = 2, scale: float = 1.0) -> SOCPModel:
     return model
 
 
+def qp_csr(seed: int = 4, n: int = 3000, density: float = 0.01) -> SOCPModel:
+    """QP-SOCP with a general sparse CSR Q that has off-diagonal entries:
+    Q = B'B + diag(d), B an (n/4) x n matrix with 3 nonzeros per column
+    (N(0,1) values) and d ~ U(0.01, 1), so Q is positive definite with about
+    9 off-diagonal entries per row.  n/2 boxed variables in [-10, 10], the
+    rest in cones of 20; A1 (n/2 rows) and A2 (n/4 rows in cones of 25) at
+    `density`.  Q is passed as a CSR matrix, so it is scaled with A and its
+    lambda_max comes from the power iteration (not from its diagonal).  The
+    planted dual makes the problem bounded: c = A'y0 + z0 - Q x0."""
+    rng = np.random.default_rng(seed)
+    n_cone = (n // 2) // 20 * 20
+    n_box = n - n_cone
+    var_dims = [20] * (n_cone // 20)
+    m1 = n // 2
+    m2 = (n // 4) // 25 * 25
+    A1 = sp.random(m1, n, density=density, random_state=rng, data_rvs=rng.standard_normal, format="csr")
+    A2 = sp.random(m2, n, density=density, random_state=rng, data_rvs=rng.standard_normal, format="csr")
+    model = _assemble(rng, A1, A2, n_box, var_dims, [25] * (m2 // 25))
+    k = max(1, n // 4)
+    rows = rng.integers(0, k, size=3 * n)
+    cols = np.repeat(np.arange(n), 3)
+    B = sp.csr_matrix((rng.standard_normal(3 * n), (rows, cols)), shape=(k, n))
+    Q = (B.T @ B + sp.diags(rng.uniform(0.01, 1.0, size=n))).tocsr()
+    model.Q = Q
+    model.c = model.c - Q @ model.planted["x0"]
+    model.__post_init__()
+    return model
+
+
 def small_socp(seed: int, n: int = None, diag_q: bool = None) -> SOCPModel:
     """One instance of the serving stream: n lognormal (median 400, 50..20000),
     m ~ n/2, density 2-5%, 1-200 variable cones of size 3-64, and for half of

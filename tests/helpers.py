@@ -79,3 +79,30 @@ def tall_model(seed=3):
     A2 = sp.random(int(np.sum(con_dims)), n, density=0.03, random_state=rng, data_rvs=rng.standard_normal,
                    format="csr")
     return instances._assemble(rng, A1, A2, n_box, var_dims, con_dims)
+
+
+def cone_branches(bar, dual, starts):
+    """Projection branch of every cone from a full iteration's outputs: 0 when
+    the projection is the origin (bar block all zero), 1 when the raw point
+    was inside the cone (dual block all zero: bar = raw exactly), 2 for a
+    projection onto the boundary.  Variable cones: (x_bar, z_bar); constraint
+    cones: (s, y_bar).  The branches set these blocks to exact zeros, so the
+    test is exact."""
+    starts = np.asarray(starts, dtype=np.int64)
+    if len(starts) < 2 or starts[-1] <= starts[0]:
+        return np.zeros(0, dtype=np.int8)
+    lo, hi = int(starts[0]), int(starts[-1])
+    idx = starts[:-1] - lo
+    nb = np.add.reduceat(np.abs(bar[lo:hi]) > 0, idx)
+    nd = np.add.reduceat(np.abs(dual[lo:hi]) > 0, idx)
+    return np.where(nb == 0, 0, np.where(nd == 0, 1, 2)).astype(np.int8)
+
+
+def branch_disagreements(g, o, model):
+    """Cones whose projection branch differs between the CUDA path (g) and
+    the oracle (o) after a full iteration: (variable cones, constraint cones)."""
+    vx = np.sum(cone_branches(g.get("x_bar"), g.get("z_bar"), model.SOC_var_idx) !=
+                cone_branches(o.get("x_bar"), o.get("z_bar"), model.SOC_var_idx))
+    cy = np.sum(cone_branches(g.get("s"), g.get("y_bar"), model.SOC_con_idx) !=
+                cone_branches(o.get("s"), o.get("y_bar"), model.SOC_con_idx))
+    return int(vx), int(cy)

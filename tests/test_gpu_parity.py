@@ -8,7 +8,7 @@ the objective within 1e-6 relative of the oracle's.
 import numpy as np
 import pytest
 
-from helpers import rel_err, stress_model, tall_model
+from helpers import branch_disagreements, rel_err, stress_model, tall_model
 from hprsocp_b200 import HPRSOCP_parameters, instances
 from oracle_ctx import OracleContext
 
@@ -29,7 +29,12 @@ def models():
             # Q = D + F'F applied as an operator (no scaling, as the reference
             # does for operator Q)
             "config2_small": instances.config2(2, scale=0.01),
-            "tall": tall_model(3)}
+            "tall": tall_model(3),
+            # general sparse Q with off-diagonal entries, scaled with A; the
+            # first runs on the multi-CTA engine, the second on the
+            # single-CTA kernel
+            "qp_csr": instances.qp_csr(4, n=3000),
+            "qp_csr_small": instances.qp_csr(6, n=400, density=0.03)}
 
 
 def _pair(model):
@@ -42,9 +47,11 @@ def _setup(o, g, params=None):
     so = o.scale(params)
     sg = g.scale(params)
     lam = o.power_A() * 1.05
-    # operator Q (D + F'F): lambda_max(Q) by the power iteration, injected
-    # identically on both sides; CSR Q keeps 0 (its factors use diag(Q))
-    lamq = o.power_Q() * 1.05 if getattr(o.model, "F", None) is not None else 0.0
+    # operator Q (D + F'F) and a non-diagonal CSR Q: lambda_max(Q) by the
+    # power iteration, injected identically on both sides; a diagonal CSR Q
+    # keeps 0 (its factors use diag(Q))
+    general_q = getattr(o.model, "F", None) is not None or not so["Q_is_diag"]
+    lamq = o.power_Q() * 1.05 if general_q else 0.0
     sigma = so["norm_b"] / so["norm_c"] if so["norm_c"] > 1e-16 else 1.0
     for c in (o, g):
         c.set_sigma_lambda(sigma, lam, lamq)
@@ -70,7 +77,7 @@ def test_scaling_parity(models, name):
 
 
 @pytest.mark.parametrize("name", ["config0", "stress", "config1_small", "small_noq", "small_q", "config2_small",
-                                  "tall"])
+                                  "tall", "qp_csr", "qp_csr_small"])
 @pytest.mark.parametrize("K", [1, 150, 1000])
 def test_iterate_parity(models, name, K):
     o, g = _pair(models[name])
@@ -81,6 +88,26 @@ def test_iterate_parity(models, name, K):
         e = rel_err(g.get(v), o.get(v))
         assert e <= ITER_TOL, (name, K, v, e)
     assert g.scalars()[3] == o.scalars()[3] == K
+    # the last (full) iteration took the same projection branch on every cone
+    assert branch_disagreements(g, o, models[name]) == (0, 0)
+
+
+@pytest.mark.parametrize("name", ["config0", "stress", "qp_csr"])
+def test_cone_branches_agree_every_iteration(models, name):
+    """The harness's cone-branch report: after each of 150 single full
+    iterations, the number of cones whose projection branch differs between
+    the CUDA path and the oracle (variable cones, constraint cones)."""
+    o, g = _pair(models[name])
+    _setup(o, g)
+    counts = []
+    for _ in range(150):
+        o.iterate(1, True)
+        g.iterate(1, True)
+        counts.append(branch_disagreements(g, o, models[name]))
+    print(name, "branch disagreements per iteration:", sorted(set(counts)))
+    assert all(c == (0, 0) for c in counts), [i for i, c in enumerate(counts) if c != (0, 0)][:10]
+    for v in VECS:
+        assert rel_err(g.get(v), o.get(v)) <= ITER_TOL, v
 
 
 def test_single_iteration_agrees_to_rounding(models):
@@ -105,7 +132,7 @@ def test_single_iteration_agrees_to_rounding(models):
     assert same > 0
 
 
-@pytest.mark.parametrize("name", ["config0", "stress", "tall", "config2_small"])
+@pytest.mark.parametrize("name", ["config0", "stress", "tall", "config2_small", "qp_csr"])
 def test_residual_mnorm_sigma_parity(models, name):
     o, g = _pair(models[name])
     _setup(o, g)
@@ -143,6 +170,18 @@ def test_power_iteration_parity(models, name):
     assert abs(lo - lg) <= 1e-6 * lo
 
 
+@pytest.mark.parametrize("name", ["qp_csr", "config2_small"])
+def test_power_iteration_q_parity(models, name):
+    """lambda_max(Q) of a non-diagonal CSR Q (scaled) and of the D + F'F
+    operator (unscaled)."""
+    o, g = _pair(models[name])
+    p = HPRSOCP_parameters(verbose=False)
+    o.scale(p)
+    g.scale(p)
+    lo, lg = o.power_Q(), g.power_Q()
+    assert abs(lo - lg) <= 1e-6 * lo
+
+
 def test_solve_parity_config0(models):
     p = HPRSOCP_parameters(verbose=False, stoptol=1e-6, max_iter=100000)
     o, g = _pair(models["config0"])
@@ -163,7 +202,7 @@ def test_solve_is_deterministic(models):
     assert np.array_equal(r1.x, r2.x) and np.array_equal(r1.y, r2.y)
 
 
-@pytest.mark.parametrize("name", ["small_noq", "small_q", "config2_small", "tall"])
+@pytest.mark.parametrize("name", ["small_noq", "small_q", "config2_small", "tall", "qp_csr", "qp_csr_small"])
 def test_solve_parity_small(models, name):
     p = HPRSOCP_parameters(verbose=False, stoptol=1e-6, max_iter=100000)
     o, g = _pair(models[name])
