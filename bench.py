@@ -213,7 +213,7 @@ def run_reference(args, model, budget_s=150.0):
     print(json.dumps(line))
 
 
-def run_serving(args):
+def serving_measure(requests, slots=32, rate=0.0, baseline=60, resident=True, seed=11):
     """Serving stream: small SOCPs (n lognormal, median 400) with per-request
     tolerances 1e-4 / 1e-6 through the continuous-batching server, against
     the same requests solved one at a time with hpr_optimize."""
@@ -223,12 +223,12 @@ def run_serving(args):
     import numpy as np
     from hprsocp_b200 import HPRSOCP_parameters, _abi, instances
     from hprsocp_b200.serving import Server
-    stream = instances.serving_stream(11, args.requests, rate=args.rate)
+    stream = instances.serving_stream(seed, requests, rate=rate)
     params = [HPRSOCP_parameters(verbose=False, stoptol=tol, max_iter=200000) for _, tol, _ in stream]
     lib = _abi.load_library()
     # the server: requests submitted at their arrival times (all at t = 0 at
     # saturation), results polled in submission order
-    with Server(slots=args.slots) as srv:
+    with Server(slots=slots, resident=resident) as srv:
         for model, p in zip([m for m, _, _ in stream[:2]], params[:2]):   # warm the slots
             srv.poll(srv.submit(model, p))
         tickets = []
@@ -245,11 +245,12 @@ def run_serving(args):
             iters.append(r.iter)
             ok += r.status == "OPTIMAL"
         wall = time.perf_counter() - t0
-    rate = len(stream) / wall
+        phases = srv.phase_times()
+    rate_s = len(stream) / wall
     # one at a time, after the server (so both run with the CUDA context up
     # and the schedule autotuner's choices made): the first `baseline`
     # requests, each a full hpr_optimize, after one untimed solve
-    nb = min(args.baseline, len(stream))
+    nb = min(baseline, len(stream))
 
     def solve_one(model, p):
         prob, pc = model.to_c(), p.to_c()
@@ -265,20 +266,31 @@ def run_serving(args):
         solve_one(model, p)
     seq_rate = nb / (time.perf_counter() - t0)
     lats = np.sort(np.asarray(lats))
-    line = {"metric": "solves/s", "value": rate, "unit": "solves/s", "n_gpus": 1, "steps": len(stream),
-            "warmup": 2, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded serving stream, seed 11)",
-            "config": {"workload": "serving stream of small SOCPs: n lognormal (median 400, 50..20000), "
-                                   "m = n/2, density 2-5%, 1-200 variable cones of 3-64, half with diagonal Q, "
-                                   "tolerance 1e-4 or 1e-6 per request",
-                       "slots": args.slots, "arrival_rate": args.rate or "saturation (all at t=0)"},
+    return {"solves_per_s": rate_s, "requests": len(stream), "slots": slots,
+            "device_resident_loop": bool(resident),
+            "arrival_rate": rate or "saturation (all at t=0)",
             "latency_s": {"p50": float(np.percentile(lats, 50)), "p99": float(np.percentile(lats, 99)),
                           "max": float(lats[-1])},
             "optimal": ok, "mean_iterations": float(np.mean(iters)),
+            "mean_phase_s": phases,
             "one_at_a_time": {"value": seq_rate, "unit": "solves/s", "requests": nb,
                               "how": "hpr_optimize per request, sequentially, after the server run "
                                      "and one untimed solve"},
-            "speedup_vs_one_at_a_time": rate / seq_rate}
+            "speedup_vs_one_at_a_time": rate_s / seq_rate}
+
+
+def run_serving(args):
+    d = serving_measure(args.requests, args.slots, args.rate, args.baseline, resident=not args.host_loop)
+    line = {"metric": "solves/s", "value": d["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+            "steps": d["requests"], "warmup": 2, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded serving stream, seed 11)",
+            "config": {"workload": "serving stream of small SOCPs: n lognormal (median 400, 50..20000), "
+                                   "m = n/2, density 2-5%, 1-200 variable cones of 3-64, half with diagonal Q, "
+                                   "tolerance 1e-4 or 1e-6 per request",
+                       "slots": args.slots, "arrival_rate": d["arrival_rate"],
+                       "device_resident_loop": d["device_resident_loop"]}}
+    line.update({k: d[k] for k in ("latency_s", "optimal", "mean_iterations", "mean_phase_s", "one_at_a_time",
+                                   "speedup_vs_one_at_a_time")})
     print(json.dumps(line))
 
 
@@ -347,24 +359,6 @@ def run_spmv_baseline(args):
                       "spmv": out, "sum_ms": out["A"]["ms"] + out["AT"]["ms"]}))
 
 
-def run_gather_ceiling(args):
-    """The device's random-gather rate for a 25M-nonzero SpMV pattern (the
-    bound that a random-column SpMV meets before DRAM bandwidth), against
-    the gathers the benchmark iteration achieves."""
-    import ctypes as C
-    from hprsocp_b200 import _abi
-    lib = _abi.load_library()
-    res = {}
-    for nx in (1_500_000, 2_000_000):
-        ms, rate = C.c_double(), C.c_double()
-        rc = lib.hpr_probe_gather(0, 24_972_397, nx, C.byref(ms), C.byref(rate))
-        if rc != 0:
-            raise RuntimeError(f"hpr_probe_gather failed: {rc}")
-        res[str(nx)] = {"ms": ms.value, "gathers_per_s": rate.value}
-    print(json.dumps({"metric": "random gathers/s", "n": 24_972_397, "vector_lengths": res,
-                      "floor_ms_per_iteration": sum(r["ms"] for r in res.values())}))
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -374,12 +368,14 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the instance (testing only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", default="iterate", choices=["iterate", "serve", "tts", "spmv-baseline", "gather-ceiling"],
+    ap.add_argument("--mode", default="iterate", choices=["iterate", "serve", "tts", "spmv-baseline"],
                     help="serve: the small-SOCP serving stream; tts: time to 1e-6 per SpMV precision")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests in the stream")
     ap.add_argument("--slots", type=int, default=32, help="serve: concurrent solver slots")
     ap.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrivals/s (0 = saturation)")
     ap.add_argument("--baseline", type=int, default=60, help="serve: requests solved one at a time")
+    ap.add_argument("--host-loop", action="store_true", help="serve: keep every solve loop on the host")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.mode == "serve":
@@ -390,9 +386,6 @@ def main():
         return
     if args.mode == "spmv-baseline":
         run_spmv_baseline(args)
-        return
-    if args.mode == "gather-ceiling":
-        run_gather_ceiling(args)
         return
 
     from hprsocp_b200 import instances
@@ -484,6 +477,11 @@ def main():
                "one_thread": {"value": cpu_iteration_rate(model, iters=1, threads=1), "unit": "iter/s",
                               "cores": 1, "sample": "1 HPR iteration on one thread (the reference's CPU "
                                                     "path is single-threaded)"}}
+    serving = None
+    if not args.no_serve:
+        # a fixed 200-request sample of the serving stream (config 4) through
+        # the device-resident request loop, against one-at-a-time solves
+        serving = serving_measure(200, slots=32, baseline=30)
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "engine_config1_dram_bytes.txt")
     if os.path.exists(tfile):
@@ -505,6 +503,7 @@ def main():
         "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": clocks,
+        "serving": serving,
     }
     print(json.dumps(line))
     if dist is not None:

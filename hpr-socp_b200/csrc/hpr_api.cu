@@ -107,6 +107,11 @@ void free_all(Ctx* c) {
   c->d_con_start = c->d_var_start = nullptr;
   f(c->d_state);
   c->d_state = nullptr;
+  f(c->qop_out);
+  c->qop_out = nullptr;
+  c->q_fn = nullptr;
+  c->q_user = nullptr;
+  c->q_lam = 0.0;
   if (c->graph_partial) cudaGraphExecDestroy(c->graph_partial);
   c->graph_partial = nullptr;
   c->graph_iters = 0;
@@ -372,7 +377,14 @@ int apply_precision(Ctx* c, int mode) {
 
 }  // namespace
 
-int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
+// Everything of `solve` before its loop: scaling, the precision of the
+// stream, sigma_0, the eigenvalue estimates, the device state and the
+// initial points (solve, algorithm.jl:2765-2834).
+struct SolveSetup {
+  double sigma = 1.0, t0 = 0.0, power_time = 0.0, scaling_s = 0.0, lamA = 0.0, lamQ = 0.0;
+};
+
+int solve_setup(Ctx* c, const hpr_params* P, SolveSetup* S) {
   if (P->sigma != -1 && !(P->sigma > 0)) return set_err(c, HPR_E_BAD_INPUT, "invalid sigma");
   if (P->print_frequency != -1 && P->print_frequency <= 0) return set_err(c, HPR_E_BAD_INPUT, "invalid print_frequency");
   if (P->check_iter <= 0) return set_err(c, HPR_E_BAD_INPUT, "invalid check_iter");
@@ -401,6 +413,7 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
   }
   // compute_lambda_max_Q (unified_operations.jl:727-741)
   if (P->lambda_max_Q > 0) lamQ = P->lambda_max_Q;
+  else if (c->q_kind == HPR_Q_OPERATOR && c->q_lam > 0) lamQ = c->q_lam;
   else if (c->has_q) {
     if (c->q_kind == HPR_Q_DIAG_LOWRANK || !c->Q_is_diag) {
       HPR_TRY(launch_power_Q(c, 5000, 1e-4, &lamQ));
@@ -422,8 +435,22 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
   HPR_TRY(push_state(c));
   HPR_TRY(update_q_factors(c));
   if (P->initial_x || P->initial_y) HPR_TRY(launch_initial_points(c, P->initial_x, P->initial_y));
-  // small problems are launch-bound: replay captured partial iterations
-  if (c->A.nnz + c->n + c->m < (int64_t)4000000 && !uses_fused_iterations(c)) HPR_TRY(capture_partial_graph(c, 8));
+  S->sigma = sigma;
+  S->t0 = t0;
+  S->power_time = power_time;
+  S->scaling_s = scaling_s;
+  S->lamA = lamA;
+  S->lamQ = lamQ;
+  return HPR_OK;
+}
+
+// The loop of `solve` (algorithm.jl:2835-2905) driven from the host.
+int solve_host_loop(Ctx* c, const hpr_params* P, const SolveSetup& S, hpr_results* out) {
+  const double t0 = S.t0, power_time = S.power_time, scaling_s = S.scaling_s, lamA = S.lamA, lamQ = S.lamQ;
+  // small problems are launch-bound: replay captured partial iterations (a
+  // caller's Q operator is not captured: it may not be capturable)
+  if (c->A.nnz + c->n + c->m < (int64_t)4000000 && !uses_fused_iterations(c) && c->q_kind != HPR_Q_OPERATOR)
+    HPR_TRY(capture_partial_graph(c, 8));
   std::unique_ptr<Checkpointer, void (*)(Checkpointer*)> ckpt(nullptr, ckpt_destroy);
   if (P->auto_save) {
     int rc = HPR_OK;
@@ -473,7 +500,7 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
         if (P->verbose)
           std::printf("switching the SpMV stream to FP64 at iteration %lld (KKT %.2e)\n", (long long)iter, kkt);
         HPR_TRY(apply_precision(c, HPR_PREC_FP64));
-        if (c->A.nnz + c->n + c->m < (int64_t)4000000 && !uses_fused_iterations(c))
+        if (c->A.nnz + c->n + c->m < (int64_t)4000000 && !uses_fused_iterations(c) && c->q_kind != HPR_Q_OPERATOR)
           HPR_TRY(capture_partial_graph(c, 8));
       }
     }
@@ -550,6 +577,60 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
   }
   if (ckpt) ckpt_finish(ckpt.get());
   if (P->verbose) print_summary(status, rs, iter, tt, c->upload_s + scaling_s);
+  return HPR_OK;
+}
+
+int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
+  SolveSetup S;
+  HPR_TRY(solve_setup(c, P, &S));
+  return solve_host_loop(c, P, S, out);
+}
+
+// A solve whose loop runs on the device (one CTA of the request loop) when
+// the problem fits it, else on the host.
+int solve_resident(Ctx* c, const hpr_params* P, hpr_results* out, DQueue* q, double* phases) {
+  SolveSetup S;
+  HPR_TRY(solve_setup(c, P, &S));
+  const double t_loop = now_s();
+  if (phases) {
+    phases[0] = S.scaling_s;
+    phases[1] = S.power_time;
+  }
+  if (!q || !dsolve_eligible(c, P)) {
+    const int rc = solve_host_loop(c, P, S, out);
+    if (phases) {
+      phases[2] = now_s() - t_loop;
+      phases[3] = 0.0;  // the host loop reads back inside its own time
+    }
+    return rc;
+  }
+  hpr_results r;
+  std::memset(&r, 0, sizeof(r));
+  // the device loop's clock starts after the eigenvalue estimate
+  hpr_params Pd = *P;
+  Pd.time_limit = P->time_limit - S.power_time;
+  HPR_TRY(dqueue_solve(q, c, &Pd, S.sigma, &r));
+  // times from the start of the eigenvalue estimate, as the host loop's
+  auto shift = [&](double t) { return t + S.power_time; };
+  r.time = shift(r.time);
+  r.time_4 = shift(r.time_4);
+  r.time_6 = shift(r.time_6);
+  r.power_time = S.power_time;
+  r.lambda_max_A = S.lamA;
+  r.lambda_max_Q = S.lamQ;
+  const double t_back = now_s();
+  if (out) {
+    r.x = out->x;
+    r.y = out->y;
+    r.z = out->z;
+    r.w = out->w;
+    *out = r;
+    HPR_TRY(launch_unscale(c, out->x, out->y, out->z, out->w));
+  }
+  if (phases) {
+    phases[2] = t_back - t_loop;
+    phases[3] = now_s() - t_back;
+  }
   return HPR_OK;
 }
 
@@ -1032,6 +1113,56 @@ int hpr_set_precision(hpr_ctx* h, int mode) {
   if (mode != HPR_PREC_FP64 && mode != HPR_PREC_FP32 && mode != HPR_PREC_BF16)
     return set_err(c, HPR_E_BAD_INPUT, "unknown precision mode");
   return apply_precision(c, mode);
+}
+
+int hpr_device_memory(hpr_ctx* h, size_t* used_bytes, int64_t* allocations) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  if (used_bytes) *used_bytes = c->used;
+  if (allocations) *allocations = (int64_t)c->allocs.size();
+  return HPR_OK;
+}
+
+int hpr_set_q_operator(hpr_ctx* h, hpr_q_apply_fn apply, void* user, double lambda_max_Q) {
+  if (!h) return HPR_E_BAD_INPUT;
+  Ctx* c = C(h);
+  HPR_TRY(need_upload(c));
+  if (!apply) return set_err(c, HPR_E_BAD_INPUT, "null Q operator");
+  if (!(lambda_max_Q >= 0.0) || !std::isfinite(lambda_max_Q))
+    return set_err(c, HPR_E_BAD_INPUT, "lambda_max_Q must be finite and >= 0");
+  if (c->q_kind != HPR_Q_NONE && c->q_kind != HPR_Q_OPERATOR)
+    return set_err(c, HPR_E_STATE, "the uploaded problem already has a Q");
+  if (c->scaled) return set_err(c, HPR_E_STATE, "set the Q operator before scaling");
+  cudaSetDevice(c->device);
+  const int64_t n = c->n;
+  if (c->q_kind == HPR_Q_NONE) {
+    // the n x n identity: the Q-path epilogues run over the operator's output
+    vector<int32_t> rp((size_t)n + 1), ci((size_t)n);
+    vector<double> one((size_t)n, 1.0);
+    for (int64_t i = 0; i <= n; ++i) rp[i] = (int32_t)i;
+    for (int64_t i = 0; i < n; ++i) ci[i] = (int32_t)i;
+    hpr_csr I{n, n, n, rp.data(), ci.data(), one.data()};
+    vector<int32_t> qrp;
+    HPR_TRY(upload_csr(c, I, 0, n, n, "Q operator identity", c->Q, qrp));
+    const vector<int64_t> vcones = c->h_var_idx.size() > 1 ? c->h_var_idx : vector<int64_t>();
+    build_plan(qrp, n, vcones, c->planQ);
+    HPR_TRY(upload_plan(c, c->planQ));
+    HPR_TRY(dev_alloc_n(c, &c->qop_out, n));
+  }
+  c->q_kind = HPR_Q_OPERATOR;
+  c->has_q = true;
+  c->Q_is_diag = false;
+  c->q_fn = apply;
+  c->q_user = user;
+  c->q_lam = lambda_max_Q;
+  if (c->graph_partial) {
+    cudaGraphExecDestroy(c->graph_partial);
+    c->graph_partial = nullptr;
+    c->graph_iters = 0;
+  }
+  HPR_TRY(prepare_engine(c));
+  HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+  return HPR_OK;
 }
 
 int hpr_set_schedule(hpr_ctx* h, int mode) {

@@ -733,15 +733,16 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
 
 constexpr int kEngineSmem = kWarpsPerCta * (int)sizeof(WarpSmem);
 
-// Shared-memory carveout of every engine kernel, in percent of the 228 KB
-// shared-memory maximum: room for exactly HPR_ENGINE_MINB CTAs (with the
-// 1 KB each CTA reserves), so the rest of the SM's 256 KB stays L1.  The
-// kernel needs that L1 (the in-flight gathers and streams land there):
-// left to the driver, epilogues light enough on registers for a fourth CTA
-// get a 228 KB carveout and run a third slower.
+// Shared-memory carveout of an engine kernel, in percent of the 228 KB
+// shared-memory maximum: room for exactly the CTAs per SM its register
+// budget allows (EngineMinBlocks, with the 1 KB each CTA reserves), so the
+// rest of the SM's 256 KB stays L1, where the in-flight gathers and streams
+// land.
 #ifndef HPR_ENGINE_CARVEOUT
-#define HPR_ENGINE_CARVEOUT (((HPR_ENGINE_MINB) * (kEngineSmem + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024))
+#define HPR_ENGINE_CARVEOUT -1  // >= 0: one fixed carveout for every epilogue
 #endif
+// room for exactly `ctas` CTAs per SM (with the 1 KB each reserves)
+constexpr int engine_carveout(int ctas) { return (ctas * (kEngineSmem + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024); }
 
 // CTAs per SM requested from the register allocator, and nonzeros per lane
 // per gather round, per epilogue (an epilogue specialises these where its

@@ -361,6 +361,17 @@ struct EpiPow {
   __device__ double cone_raw(int64_t, double v, const In&, Red&) { return v; }
   __device__ void cone_apply(int64_t, double, double, double, bool, const In&, Red&) {}
 };
+#ifndef HPR_ENGINE_MINB_POW
+#define HPR_ENGINE_MINB_POW HPR_ENGINE_MINB  // CTAs per SM of the power iteration's products
+#endif
+template <>
+struct EngineMinBlocks<EpiScale> {
+  static constexpr int value = HPR_ENGINE_MINB_POW;
+};
+template <>
+struct EngineMinBlocks<EpiPow> {
+  static constexpr int value = HPR_ENGINE_MINB_POW;
+};
 
 // Dual residual in original coordinates: compute_Rd_kernel! /
 // compute_Rd_noQ_kernel! (kernels.jl:6467-6512) with the objective dots of

@@ -230,6 +230,13 @@ struct Ctx {
   double* ftmp = nullptr;   // F v (k)
   double* ftmp2 = nullptr;  // F w_bar (k)
   double* vtmp_n = nullptr;
+  // user Q operator (HPR_Q_OPERATOR): Q v by the caller's callback into
+  // qop_out; Q / planQ hold the n x n identity so that the Q-path epilogues
+  // run over the callback's output
+  hpr_q_apply_fn q_fn = nullptr;
+  void* q_user = nullptr;
+  double q_lam = 0.0;
+  double* qop_out = nullptr;
   double* vtmp_m = nullptr;
   float* g32_n = nullptr;  // FP32 copies of gathered vectors (x_hat/tempv, y)
   float* g32_m = nullptr;
@@ -317,6 +324,22 @@ int upload_csr(Ctx* c, const hpr_csr& s, int base, int64_t nr, int64_t nc, const
 int transpose_csr(Ctx* c, const DevCSR& M, DevCSR& T, std::vector<int32_t>& trp);
 // scaling (hpr_scale.cu)
 int run_scaling(Ctx* c, const hpr_params* p, hpr_scale_info* out);
+
+// device-resident solve loop and the serving request loop (hpr_dsolve.cu)
+struct DQueue;
+// true when the problem's whole solve loop can run in one CTA
+bool dsolve_eligible(const Ctx* c, const hpr_params* P);
+// the request loop on `device` with `ctas` CTAs (0: one per SM) and a ring of
+// `cap` requests; null with *err set on failure
+DQueue* dqueue_create(int device, int ctas, int cap, std::string* err);
+void dqueue_destroy(DQueue* q);
+// hand a prepared context to the request loop and wait for its solve; fills
+// the scalars of `out` (not the vectors)
+int dqueue_solve(DQueue* q, Ctx* c, const hpr_params* P, double sigma0, hpr_results* out);
+// solve with the loop on the device when the problem fits (hpr_api.cu);
+// phases (may be null) receives the wall seconds of scaling, the eigenvalue
+// estimate, the loop and the unscaled read-back
+int solve_resident(Ctx* c, const hpr_params* P, hpr_results* out, DQueue* q, double* phases = nullptr);
 
 // auto-save of the current and best iterates (hpr_checkpoint.cu)
 struct Checkpointer;

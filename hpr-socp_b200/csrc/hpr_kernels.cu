@@ -187,7 +187,7 @@ int prepare_engine(Ctx* c) {
   if (!c->uploaded) return HPR_OK;
   HPR_TRY(ensure_tiled(c, c->AT, c->planX));
   HPR_TRY(ensure_tiled(c, c->A, c->planY));
-  if (c->q_kind == HPR_Q_CSR) HPR_TRY(ensure_tiled(c, c->Q, c->planQ));
+  if (c->q_kind == HPR_Q_CSR || c->q_kind == HPR_Q_OPERATOR) HPR_TRY(ensure_tiled(c, c->Q, c->planQ));
   if (c->q_kind == HPR_Q_DIAG_LOWRANK) {
     HPR_TRY(ensure_tiled(c, c->F, c->planF));
     HPR_TRY(ensure_tiled(c, c->FT, c->planQ));
@@ -208,8 +208,9 @@ int engine_grid(int* smem_bytes) {
   std::call_once(once, [] {
     auto k = engine_kernel<Epi, PREC>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-    if (HPR_ENGINE_CARVEOUT >= 0)
-      cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, (int)(HPR_ENGINE_CARVEOUT));
+    const int carve = HPR_ENGINE_CARVEOUT >= 0 ? (int)(HPR_ENGINE_CARVEOUT)
+                                               : engine_carveout(EngineMinBlocks<Epi>::value);
+    cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
     int per_sm = 0, dev = 0, sms = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kEngineThreads, dyn);
     cudaGetDevice(&dev);
@@ -296,6 +297,14 @@ int qmap(Ctx* c, const double* v, double* out, double* tmp) {
     return engine_launch(c, c->FT, c->planQ, c->d_var_start, tmp, nullptr, plain(out, c->qdiag, v), false, false,
                          0);
   }
+  if (c->q_kind == HPR_Q_OPERATOR) {
+    // the caller's Q v, enqueued on the context stream (Qmap! of a user
+    // AbstractQOperator)
+    c->q_fn(c->q_user, v, out, c->n, (void*)c->stream);
+    c->launches++;
+    HPR_CUDA(c, cudaGetLastError());
+    return HPR_OK;
+  }
   HPR_CUDA(c, cudaMemsetAsync(out, 0, c->n * sizeof(double), c->stream));
   return HPR_OK;
 }
@@ -372,6 +381,10 @@ int launch_iteration(Ctx* c, bool full) {
   if (lowrank) {
     HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, c->w, nullptr, plain(c->ftmp), false, false, 0));
     HPR_TRY(engine_launch(c, c->FT, c->planQ, c->d_var_start, c->ftmp, nullptr, E.eq, false, false, 0));
+  } else if (c->q_kind == HPR_Q_OPERATOR) {
+    // Q w from the caller's operator; the epilogue runs over the identity
+    HPR_TRY(qmap(c, c->w, c->qop_out, nullptr));
+    HPR_TRY(engine_launch(c, c->Q, c->planQ, c->d_var_start, c->qop_out, nullptr, E.eq, false, false, 0));
   } else {
     HPR_TRY(engine_launch(c, c->Q, c->planQ, c->d_var_start, c->w, nullptr, E.eq, false, false, 0));
   }
@@ -379,6 +392,9 @@ int launch_iteration(Ctx* c, bool full) {
     if (lowrank) {
       HPR_TRY(engine_launch(c, c->F, c->planF, nullptr, c->w_bar, nullptr, plain(c->ftmp2), false, false, 0));
       HPR_TRY(engine_launch(c, c->FT, c->planQ, c->d_var_start, c->ftmp2, nullptr, E.et, false, false, 0));
+    } else if (c->q_kind == HPR_Q_OPERATOR) {
+      HPR_TRY(qmap(c, c->w_bar, c->qop_out, nullptr));
+      HPR_TRY(engine_launch(c, c->Q, c->planQ, c->d_var_start, c->qop_out, nullptr, E.et, false, false, 0));
     } else {
       HPR_TRY(engine_launch(c, c->Q, c->planQ, c->d_var_start, c->w_bar, nullptr, E.et, false, false, 0));
     }
@@ -455,7 +471,7 @@ int launch_fused_prec(Ctx* c, const FStage<E0>& s0, const FStage<E1>& s1, const 
 }
 
 bool fused_eligible(const Ctx* c) {
-  if (c->q_kind == HPR_Q_DIAG_LOWRANK) return false;
+  if (c->q_kind == HPR_Q_DIAG_LOWRANK || c->q_kind == HPR_Q_OPERATOR) return false;
   auto fits = [](const Plan& p) { return (int64_t)p.tasks.size() <= kFusedMaxTiles; };
   if (!fits(c->planX) || !fits(c->planY)) return false;
   // with Q the reduced-precision streams apply to A only; keep those unfused

@@ -301,7 +301,7 @@ int run_scaling(Ctx* c, const hpr_params* p, hpr_scale_info* out) {
     HPR_TRY(vec_map(c, m, [=] __device__(int64_t i) { rn[i] = 1.0; }));
     HPR_TRY(vec_map(c, n, [=] __device__(int64_t i) { cn[i] = 1.0; }));
   }
-  if (c->q_kind == HPR_Q_DIAG_LOWRANK) {
+  if (c->q_kind == HPR_Q_DIAG_LOWRANK || c->q_kind == HPR_Q_OPERATOR) {
     // operator Q: no scaling at all (scaling.jl:800-846)
     c->b_scale = c->c_scale = 1.0;
     c->norm_b = m > 0 ? jmax(nl2[0], ninf[1]) : 0.0;

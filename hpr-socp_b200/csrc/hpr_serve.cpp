@@ -8,8 +8,14 @@
 // memory free up, and the kernels of all running solves overlap on the
 // device (small problems launch only the CTAs their tiles need).  Each
 // request carries its own parameters, so each retires at its own tolerance.
-// A solve inside the server is exactly hpr_upload + hpr_solve on a private
-// context, so its result is bit-identical to solving it alone.
+// A request is uploaded, scaled and its eigenvalues estimated on the slot's
+// private context.  When the problem fits one CTA (hpr_dsolve.cu), its whole
+// solve loop then runs inside the device-resident request loop: one
+// persistent kernel whose CTAs each solve one request at a time, so the
+// loops of many requests run in one launch with no host round trip per
+// residual check.  Larger problems run the host-driven loop of hpr_solve.
+// Either way a request's result does not depend on the other requests: the
+// same request gives the same bits alone and in the mix.
 //
 // The reference solves one model per `optimize` call (src/algorithm.jl:
 // 2538-2581) and its dataset runner loops over files one at a time
@@ -31,7 +37,7 @@
 
 #include <cuda_runtime.h>
 
-#include "../../include/hprsocp_b200.h"
+#include "hpr_internal.h"
 
 namespace {
 
@@ -147,6 +153,12 @@ struct hpr_server {
   int64_t running = 0;
   bool stop = false;
   std::string err;
+  hpr::DQueue* dq = nullptr;  // device-resident request loop (null: host loops only)
+  int resident = 1;
+  // wall seconds summed over finished requests: queue wait, upload, scaling,
+  // eigenvalue estimate, solve loop, unscaled read-back
+  double phase_sum[6] = {0, 0, 0, 0, 0, 0};
+  int64_t phase_count = 0;
 
   void worker(hpr_ctx* ctx) {
     for (;;) {
@@ -174,8 +186,15 @@ struct hpr_server {
       r.params.verbose = 0;
       r.params.device_number = device;
       r.params.save_filename = r.save_filename.empty() ? nullptr : r.save_filename.c_str();
+      double ph[6] = {0, 0, 0, 0, 0, 0};
+      const double t_start = now_s();
+      ph[0] = t_start - r.t_submit;
       f.rc = hpr_upload(ctx, &r.prob->p);
-      if (f.rc == HPR_OK) f.rc = hpr_solve(ctx, &r.params, &f.res);
+      ph[1] = now_s() - t_start;
+      if (f.rc == HPR_OK) {
+        cudaSetDevice(device);
+        f.rc = hpr::solve_resident(&ctx->c, &r.params, &f.res, resident ? dq : nullptr, ph + 2);
+      }
       if (f.rc != HPR_OK) f.err = hpr_last_error(ctx);
       f.res.x = f.res.y = f.res.z = f.res.w = nullptr;
       f.latency = now_s() - r.t_submit;
@@ -185,6 +204,8 @@ struct hpr_server {
         reserved -= r.est;
         --running;
         done[r.ticket] = std::move(f);
+        for (int k = 0; k < 6; ++k) phase_sum[k] += ph[k];
+        ++phase_count;
       }
       cv_done.notify_all();
       cv_work.notify_all();
@@ -226,8 +247,22 @@ int hpr_serve_create(int device, int slots, size_t hbm_budget, hpr_server** out)
     hbm_budget = (size_t)(0.9 * (double)fr);
   }
   s->budget = hbm_budget;
+  std::string qerr;
+  s->dq = hpr::dqueue_create(device, 0, 4096, &qerr);
+  if (!s->dq) {
+    for (hpr_ctx* d : ctxs) hpr_destroy(d);
+    delete s;
+    return HPR_E_CUDA;
+  }
   for (hpr_ctx* c : ctxs) s->workers.emplace_back([s, c] { s->worker(c); });
   *out = s;
+  return HPR_OK;
+}
+
+int hpr_serve_set_resident(hpr_server* s, int on) {
+  if (!s) return HPR_E_BAD_INPUT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->resident = on ? 1 : 0;
   return HPR_OK;
 }
 
@@ -318,6 +353,14 @@ int hpr_serve_stats(hpr_server* s, int64_t* queued, int64_t* running, size_t* re
   return HPR_OK;
 }
 
+int hpr_serve_phase_times(hpr_server* s, double* seconds, int64_t* requests) {
+  if (!s || !seconds) return HPR_E_BAD_INPUT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (int k = 0; k < 6; ++k) seconds[k] = s->phase_sum[k];
+  if (requests) *requests = s->phase_count;
+  return HPR_OK;
+}
+
 const char* hpr_serve_last_error(hpr_server* s) { return s ? s->err.c_str() : "null server"; }
 
 int hpr_serve_destroy(hpr_server* s) {
@@ -329,6 +372,7 @@ int hpr_serve_destroy(hpr_server* s) {
   s->cv_work.notify_all();
   s->cv_done.notify_all();
   for (std::thread& t : s->workers) t.join();
+  hpr::dqueue_destroy(s->dq);
   delete s;
   return HPR_OK;
 }

@@ -26,6 +26,7 @@ HPR_E_UNSUPPORTED = 7
 HPR_Q_NONE = 0
 HPR_Q_CSR = 1
 HPR_Q_DIAG_LOWRANK = 2
+HPR_Q_OPERATOR = 3
 
 HPR_BC_NORM = {"l2": 0, "rms": 1, "linf": 2, "l_inf": 2, "inf": 2}
 
@@ -146,17 +147,20 @@ PROTOTYPES = {
     "hpr_set_vector": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_size_t]),
     "hpr_get_solution": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
     "hpr_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "hpr_set_q_operator": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),
+    "hpr_device_memory": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), _lp]),
     "hpr_set_schedule": (C.c_int, [C.c_void_p, C.c_int]),
     "hpr_solve": (C.c_int, [C.c_void_p, C.POINTER(hpr_params), C.POINTER(hpr_results)]),
     "hpr_optimize": (C.c_int, [C.POINTER(hpr_problem), C.POINTER(hpr_params),
                                C.POINTER(hpr_results)]),
     "hpr_last_iterate_ms": (C.c_int, [C.c_void_p, _dp, _lp]),
     "hpr_iteration_bytes": (C.c_int, [C.c_void_p, _dp]),
-    "hpr_probe_gather": (C.c_int, [C.c_int, C.c_int64, C.c_int64, _dp, _dp]),
     "hpr_serve_create": (C.c_int, [C.c_int, C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]),
     "hpr_serve_submit": (C.c_int, [C.c_void_p, C.POINTER(hpr_problem), C.POINTER(hpr_params), _lp]),
     "hpr_serve_poll": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.POINTER(hpr_results), _dp]),
+    "hpr_serve_set_resident": (C.c_int, [C.c_void_p, C.c_int]),
     "hpr_serve_stats": (C.c_int, [C.c_void_p, _lp, _lp, C.POINTER(C.c_size_t)]),
+    "hpr_serve_phase_times": (C.c_int, [C.c_void_p, _dp, _lp]),
     "hpr_serve_last_error": (C.c_char_p, [C.c_void_p]),
     "hpr_serve_destroy": (C.c_int, [C.c_void_p]),
     "hpr_cbf_read": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),

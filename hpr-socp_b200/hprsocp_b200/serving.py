@@ -16,7 +16,7 @@ class Server:
     """`slots` solver contexts on one device; requests are admitted while
     their estimated device memory fits `hbm_budget` bytes (0 = 90% of free)."""
 
-    def __init__(self, slots: int = 16, device: int = 0, hbm_budget: int = 0):
+    def __init__(self, slots: int = 16, device: int = 0, hbm_budget: int = 0, resident: bool = True):
         self.lib = _abi.load_library()
         h = C.c_void_p()
         rc = self.lib.hpr_serve_create(device, slots, hbm_budget, C.byref(h))
@@ -24,6 +24,9 @@ class Server:
             raise _abi.HPRError(rc, self.lib.hpr_status_string(rc).decode())
         self.h = h
         self._shapes = {}
+        # resident: small problems run their whole solve loop in the
+        # device-resident request loop; False keeps every loop on the host
+        self.lib.hpr_serve_set_resident(self.h, 1 if resident else 0)
 
     def _err(self, rc):
         msg = self.lib.hpr_serve_last_error(self.h).decode() if self.h else ""
@@ -60,6 +63,15 @@ class Server:
         q, run, res = C.c_int64(), C.c_int64(), C.c_size_t()
         self.lib.hpr_serve_stats(self.h, C.byref(q), C.byref(run), C.byref(res))
         return {"queued": q.value, "running": run.value, "reserved_bytes": res.value}
+
+    def phase_times(self):
+        """Mean wall seconds per finished request: queue wait, upload,
+        scaling, eigenvalue estimate, solve loop, read-back."""
+        sec = (C.c_double * 6)()
+        n = C.c_int64()
+        self.lib.hpr_serve_phase_times(self.h, sec, C.byref(n))
+        names = ("queue_wait", "upload", "scaling", "power_iteration", "solve_loop", "readback")
+        return {k: (sec[i] / n.value if n.value else 0.0) for i, k in enumerate(names)}
 
     def close(self):
         if getattr(self, "h", None):

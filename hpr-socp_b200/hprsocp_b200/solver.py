@@ -205,6 +205,12 @@ class Context:
     def iterate(self, k: int, full_last: bool = True):
         self._check(self.lib.hpr_iterate(self.h, k, int(full_last)))
 
+    def device_memory(self):
+        """(bytes held within the HBM budget, live device allocations)."""
+        used, n = C.c_size_t(), C.c_int64()
+        self._check(self.lib.hpr_device_memory(self.h, C.byref(used), C.byref(n)))
+        return used.value, n.value
+
     def last_iterate(self):
         ms = C.c_double()
         n = C.c_int64()

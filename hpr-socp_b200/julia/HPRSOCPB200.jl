@@ -21,6 +21,7 @@ const LIB = Ref{String}(joinpath(@__DIR__, "..", "lib", "libhprsocp_b200.so"))
 const HPR_Q_NONE = Int32(0)
 const HPR_Q_CSR = Int32(1)
 const HPR_Q_DIAG_LOWRANK = Int32(2)
+const HPR_Q_OPERATOR = Int32(3)
 
 const BC_NORM = Dict(:l2 => Int32(0), :rms => Int32(1), :linf => Int32(2), :l_inf => Int32(2), :inf => Int32(2))
 const SOC_STRATEGY = Dict(
@@ -205,11 +206,35 @@ function c_problem(model, keep::Vector{Any})
         qd = pointer(push!(keep, Vector{Float64}(model.Q.d))[end])
         k = size(model.Q.F, 1)
         F = csr_of_transpose(sparse(transpose(model.Q.F)), k, n, keep)
-    elseif model.Q !== nothing
-        error("HPRSOCPB200 supports a sparse Q or DiagPlusLowRankQ, got $(typeof(model.Q))")
+    elseif model.Q !== nothing && !is_user_operator(model.Q)
+        error("HPRSOCPB200 supports a sparse Q, DiagPlusLowRankQ or a user Q operator, got $(typeof(model.Q))")
     end
     return CProblem(m, n, model.number_linear_con, model.number_lu_x, A, AT, vecs..., pointer(con), length(con),
                     pointer(var), length(var), Int32(1), qkind, Q, qd, F, model.obj_constant)
+end
+
+# ---- a user Q operator (src/Q_operators/Q_operator_interface.jl:32-151) ---
+# A model whose Q is a user AbstractQOperatorCPU keeps q_kind NONE in the
+# upload; the library then calls back into Julia for every product Q v
+# (hpr_set_q_operator).  The callback views the library's device vectors as
+# CuArrays (CUDA.jl, loaded by the caller) and runs the operator's GPU form,
+# made once by the reference's to_gpu, through its Qmap!(x, Qx, Q), on the
+# stream the library passes in.
+is_user_operator(Q) = isdefined(Main, :HPRSOCP) && Q isa Main.HPRSOCP.AbstractQOperatorCPU
+
+struct QOperatorBox
+    gpu::Any  # the operator's GPU form (to_gpu)
+end
+
+function q_apply(user::Ptr{Cvoid}, vin::Ptr{Float64}, vout::Ptr{Float64}, n::Int64, stream::Ptr{Cvoid})::Cvoid
+    box = unsafe_pointer_to_objref(user)::QOperatorBox
+    CUDA = Main.CUDA
+    x = unsafe_wrap(CUDA.CuArray, CUDA.CuPtr{Float64}(UInt(vin)), Int(n); own = false)
+    Qx = unsafe_wrap(CUDA.CuArray, CUDA.CuPtr{Float64}(UInt(vout)), Int(n); own = false)
+    CUDA.stream!(CUDA.CuStream(reinterpret(CUDA.CUstream, stream))) do
+        Main.HPRSOCP.Qmap!(x, Qx, box.gpu)
+    end
+    return nothing
 end
 
 function check(rc::Integer)
@@ -235,10 +260,28 @@ function optimize(model, params, Results::Type)
     x, y, z, w = zeros(n), zeros(m), zeros(n), zeros(n)
     res = CResults()
     res.x, res.y, res.z, res.w = pointer(x), pointer(y), pointer(z), pointer(w)
-    GC.@preserve keep x y z w begin
-        rc = ccall((:hpr_optimize, LIB[]), Cint, (Ref{CProblem}, Ref{CParams}, Ref{CResults}), prob, p, res)
+    if model.Q !== nothing && is_user_operator(model.Q)
+        # context, upload, the operator, solve (hpr_optimize has no operator)
+        box = QOperatorBox(Main.HPRSOCP.to_gpu(model.Q))
+        fn = @cfunction(q_apply, Cvoid, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int64, Ptr{Cvoid}))
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:hpr_create, LIB[]), Cint, (Cint, Csize_t, Ref{Ptr{Cvoid}}), Cint(params.device_number), 0, h))
+        try
+            GC.@preserve keep x y z w box begin
+                check(ccall((:hpr_upload, LIB[]), Cint, (Ptr{Cvoid}, Ref{CProblem}), h[], prob))
+                check(ccall((:hpr_set_q_operator, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Any, Cdouble), h[], fn, box,
+                            0.0))
+                check(ccall((:hpr_solve, LIB[]), Cint, (Ptr{Cvoid}, Ref{CParams}, Ref{CResults}), h[], p, res))
+            end
+        finally
+            ccall((:hpr_destroy, LIB[]), Cint, (Ptr{Cvoid},), h[])
+        end
+    else
+        GC.@preserve keep x y z w begin
+            rc = ccall((:hpr_optimize, LIB[]), Cint, (Ref{CProblem}, Ref{CParams}, Ref{CResults}), prob, p, res)
+        end
+        check(rc)
     end
-    check(rc)
     out = Results()
     out.iter, out.iter_4, out.iter_6 = res.iter, res.iter_4, res.iter_6
     out.time, out.time_4, out.time_6, out.power_time = res.time, res.time_4, res.time_6, res.power_time

@@ -61,10 +61,13 @@ typedef struct hpr_csr {
  *                 is detected as in check_Q_diagonal (src/utils/scaling.jl:1312)
  *  DIAG_LOWRANK : operator Q = diag(q_diag) + F'F, never formed.  Like the
  *                 reference's user AbstractQOperator, an operator Q disables
- *                 all scaling (src/utils/scaling.jl:800-846).                */
+ *                 all scaling (src/utils/scaling.jl:800-846).
+ *  OPERATOR     : a caller-supplied Q v on the device, set after the upload
+ *                 with hpr_set_q_operator (no scaling either).              */
 #define HPR_Q_NONE 0
 #define HPR_Q_CSR 1
 #define HPR_Q_DIAG_LOWRANK 2
+#define HPR_Q_OPERATOR 3
 
 typedef struct hpr_problem {
   int64_t m;            /* rows of A                                       */
@@ -291,7 +294,10 @@ int hpr_iterate(hpr_ctx* ctx, int64_t k, int full_last);
 /* KKT residuals of the current (x_bar, y_bar, z_bar[, w_bar]) in original
  * coordinates (compute_residuals!, algorithm.jl:113-196); include_bounds adds
  * the iteration-0 bound/cone violation (compute_bounds_violation!,
- * algorithm.jl:199-256).                                                    */
+ * algorithm.jl:199-256).  include_bounds writes the violation into the
+ * context's dx, as the reference writes ws.dx: hpr_mnorm and the restart
+ * test read dx, so use include_bounds only at iteration 0 (as the solve
+ * loop does) or before the next hpr_iterate with full_last != 0.            */
 int hpr_compute_residuals(hpr_ctx* ctx, int include_bounds,
                           hpr_residuals* out);
 
@@ -315,7 +321,9 @@ int hpr_compute_residuals(hpr_ctx* ctx, int include_bounds,
  *    get HPR_E_UNSUPPORTED with the sizes in hpr_last_error;
  *  - FP64 stream only (HPR_E_UNSUPPORTED after hpr_set_precision != 0);
  *  - nothing in the scratch has to start at zero: every slot is written
- *    before it is read, and no state survives between calls;
+ *    before it is read, and nothing in the scratch carries from one call to
+ *    the next (include_bounds writes the context's dx, exactly as
+ *    hpr_compute_residuals does: see there);
  *  - all contexts of the process share the scratch of a device, so calls
  *    that overlapped in time would overwrite each other's partial sums; the
  *    library therefore serialises the calls per device with a host lock
@@ -325,6 +333,10 @@ int hpr_compute_residuals(hpr_ctx* ctx, int include_bounds,
  *    before any stream capture.                                             */
 int hpr_compute_residuals_noalloc(hpr_ctx* ctx, int include_bounds,
                                   hpr_residuals* out);
+
+/* The context's device memory: bytes it holds within its HBM budget and the
+ * number of its live device allocations (either pointer may be NULL).     */
+int hpr_device_memory(hpr_ctx* ctx, size_t* used_bytes, int64_t* allocations);
 
 /* Restart gap measure (compute_M_norm!, algorithm.jl:1302-1359), using dx,
  * dy (and dw) from the last full iteration.                                 */
@@ -369,6 +381,21 @@ int hpr_set_schedule(hpr_ctx* ctx, int mode);
 /* Precision of the A / A' stream (HPR_PREC_*); re-packs the scaled values.  */
 int hpr_set_precision(hpr_ctx* ctx, int mode);
 
+/* A user quadratic operator, the counterpart of a user AbstractQOperator
+ * (src/Q_operators/Q_operator_interface.jl:32-151, Qmap! of
+ * src/Q_operators/sparse_matrix_operator.jl:27-51): apply(user, in, out, n,
+ * stream) must enqueue out = Q in on `stream` (a cudaStream_t) for device
+ * vectors of length n, without synchronising the device, for a symmetric
+ * positive semidefinite Q.  Call it after hpr_upload of a problem with
+ * q_kind HPR_Q_NONE and before hpr_scale or a solve: the problem becomes
+ * q_kind HPR_Q_OPERATOR, and, as in the reference, an operator Q turns
+ * scaling off.  lambda_max_Q > 0 is used as lambda_max(Q) (a solve's
+ * params.lambda_max_Q takes precedence); otherwise the power iteration
+ * estimates it through `apply`.  The operator is called from the thread
+ * that drives the context; it stays set until the next hpr_upload.        */
+typedef void (*hpr_q_apply_fn)(void* user, const double* in, double* out, int64_t n, void* stream);
+int hpr_set_q_operator(hpr_ctx* ctx, hpr_q_apply_fn apply, void* user, double lambda_max_Q);
+
 /* The whole solve (solve(), algorithm.jl:2765-2905): scaling, power
  * iteration, the restart / sigma loop and unscaling, with the same check,
  * print and termination schedule.  `res->x/y/z/w` receive the unscaled
@@ -392,13 +419,6 @@ int hpr_last_iterate_ms(hpr_ctx* ctx, double* ms_total, int64_t* launches);
  * roofline numerator used by the benchmark).                               */
 int hpr_iteration_bytes(hpr_ctx* ctx, double* bytes_per_iter);
 
-/* Diagnostic (no counterpart in the reference): the device's rate for the
- * access pattern of a random-column SpMV, n streamed (column, value) pairs
- * each gathering one double from a vector of nx entries, with no solver
- * work around it.  Returns the milliseconds of one pass and the gathers per
- * second.  Allocates its own buffers (about 12n + 8nx bytes).             */
-int hpr_probe_gather(int device, int64_t n, int64_t nx, double* ms,
-                     double* gathers_per_s);
 
 /* ------------------------------------------------------------------------ */
 /* Serving: continuous batching of many small problems on one device.       */
@@ -409,9 +429,20 @@ typedef struct hpr_server hpr_server;
 
 /* `slots` solver contexts (one stream and host thread each) on `device`;
  * requests are admitted while their estimated device memory fits
- * `hbm_budget` bytes (0 = 90% of the device's free memory).                */
+ * `hbm_budget` bytes (0 = 90% of the device's free memory).  A slot
+ * uploads, scales and estimates the eigenvalues of its request; a problem
+ * small enough for one CTA (every matrix side within the single-CTA tile
+ * limit, FP64, no operator Q, no auto-save) is then solved by the
+ * device-resident request loop: a persistent kernel, one CTA per solve,
+ * running the whole HPR loop (iterations, residual checks, restarts, sigma
+ * updates, termination) on the device.  Other requests run the host loop
+ * of hpr_solve.                                                            */
 int hpr_serve_create(int device, int slots, size_t hbm_budget,
                      hpr_server** out);
+
+/* 1 (default): eligible requests use the device-resident request loop;
+ * 0: every request runs the host loop of hpr_solve (for comparisons).     */
+int hpr_serve_set_resident(hpr_server* srv, int on);
 
 /* Queue one problem with its own parameters (tolerance, limits, precision);
  * the problem's arrays are copied, so the caller may free them on return.
@@ -430,6 +461,11 @@ int hpr_serve_poll(hpr_server* srv, int64_t ticket, int wait_ms,
 
 int hpr_serve_stats(hpr_server* srv, int64_t* queued, int64_t* running,
                     size_t* reserved_bytes);
+
+/* Wall seconds spent by the finished requests, summed, in seconds[0..5]:
+ * queue wait, upload, scaling, eigenvalue estimate, solve loop, unscaled
+ * read-back; *requests = how many requests they cover.                     */
+int hpr_serve_phase_times(hpr_server* srv, double* seconds, int64_t* requests);
 const char* hpr_serve_last_error(hpr_server* srv);
 
 /* Stops the slots after their current solves; queued requests are dropped.

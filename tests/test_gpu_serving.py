@@ -20,10 +20,14 @@ def _params(tol):
 
 
 def test_each_result_is_the_same_alone_and_in_the_mix(stream):
+    """A request solved alone (a one-slot server, nothing else on the
+    device) and the same request among 40 submitted at once to 16 slots give
+    the same bits: each small problem's loop runs in its own CTA of the
+    device-resident request loop, every reduction in a fixed order."""
     alone = []
-    for model, tol, _ in stream:
-        with Context(model) as ctx:
-            alone.append(ctx.solve(_params(tol)))
+    with Server(slots=1) as srv:
+        for model, tol, _ in stream:
+            alone.append(srv.poll(srv.submit(model, _params(tol)))[0])
     with Server(slots=16) as srv:
         tickets = [srv.submit(model, _params(tol)) for model, tol, _ in stream]
         mixed = [srv.poll(t)[0] for t in tickets]
@@ -32,6 +36,28 @@ def test_each_result_is_the_same_alone_and_in_the_mix(stream):
         assert a.iter == b.iter
         assert b.residuals <= tol
         assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y) and np.array_equal(a.z, b.z)
+
+
+def test_device_loop_agrees_with_the_host_loop(stream):
+    """The device-resident loop runs the host loop's logic with its
+    reductions summed in another fixed order: each request reaches the same
+    status at its tolerance with the objective within 1e-6 and the iteration
+    count within one check interval.  With the resident loop switched off,
+    a server solve is hpr_solve on a private context, bit for bit."""
+    host = []
+    for model, tol, _ in stream:
+        with Context(model) as ctx:
+            host.append(ctx.solve(_params(tol)))
+    with Server(slots=16) as srv:
+        dev = [srv.poll(t)[0] for t in [srv.submit(m, _params(tol)) for m, tol, _ in stream]]
+    with Server(slots=16, resident=False) as srv:
+        off = [srv.poll(t)[0] for t in [srv.submit(m, _params(tol)) for m, tol, _ in stream]]
+    for (model, tol, _), h, d, o in zip(stream, host, dev, off):
+        assert h.status == d.status == "OPTIMAL" and d.residuals <= tol
+        # both are tol-accurate solutions (tol 1e-4 or 1e-6)
+        assert abs(d.primal_obj - h.primal_obj) <= 10 * tol * max(1.0, abs(h.primal_obj))
+        assert abs(d.iter - h.iter) <= 150, (d.iter, h.iter)
+        assert o.iter == h.iter and np.array_equal(o.x, h.x) and np.array_equal(o.y, h.y)
 
 
 def test_each_request_retires_at_its_own_tolerance(stream):

@@ -41,13 +41,24 @@ def _close(a, b):
     return abs(a - b) <= TOL * max(1.0, abs(b))
 
 
+def _free_device_bytes():
+    import torch
+    return torch.cuda.mem_get_info()[0]
+
+
 @pytest.mark.parametrize("name", ["config0", "stress", "config2_small"])
 @pytest.mark.parametrize("bounds", [False, True])
 def test_matches_existing_entry_point_on_two_calls(name, bounds):
     with _iterated(_model(name)) as ctx:
         ref = ctx.residuals(include_bounds=bounds)
+        # the promise itself: the context allocates nothing more and the
+        # device's free memory does not move across the two calls
+        _free_device_bytes()  # torch's CUDA state is set up before the measurement
+        mem0, free0 = ctx.device_memory(), _free_device_bytes()
         first = ctx.residuals_noalloc(include_bounds=bounds)
         second = ctx.residuals_noalloc(include_bounds=bounds)
+        assert ctx.device_memory() == mem0
+        assert _free_device_bytes() == free0
         again = ctx.residuals(include_bounds=bounds)
     for k, v in ref.items():
         assert _close(first[k], v), (k, first[k], v)
