@@ -7,6 +7,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <thread>
 
 #include "hpr_engine.cuh"
 
@@ -588,7 +589,9 @@ int solve_loop(Ctx* c, const hpr_params* P, hpr_results* out) {
 
 // A solve whose loop runs on the device (one CTA of the request loop) when
 // the problem fits it, else on the host.
-int solve_resident(Ctx* c, const hpr_params* P, hpr_results* out, DQueue* q, double* phases) {
+int solve_resident_begin(Ctx* c, const hpr_params* P, hpr_results* out, DQueue* q, ResidentJob* job,
+                         bool* submitted, double* phases) {
+  *submitted = false;
   SolveSetup S;
   HPR_TRY(solve_setup(c, P, &S));
   const double t_loop = now_s();
@@ -598,27 +601,31 @@ int solve_resident(Ctx* c, const hpr_params* P, hpr_results* out, DQueue* q, dou
   }
   if (!q || !dsolve_eligible(c, P)) {
     const int rc = solve_host_loop(c, P, S, out);
-    if (phases) {
-      phases[2] = now_s() - t_loop;
-      phases[3] = 0.0;  // the host loop reads back inside its own time
-    }
+    if (phases) phases[2] = now_s() - t_loop;
     return rc;
   }
-  hpr_results r;
-  std::memset(&r, 0, sizeof(r));
   // the device loop's clock starts after the eigenvalue estimate
   hpr_params Pd = *P;
   Pd.time_limit = P->time_limit - S.power_time;
-  HPR_TRY(dqueue_solve(q, c, &Pd, S.sigma, &r));
+  job->power_time = S.power_time;
+  job->lamA = S.lamA;
+  job->lamQ = S.lamQ;
+  job->t_loop = t_loop;
+  HPR_TRY(dqueue_submit(q, c, &Pd, S.sigma, &job->slot));
+  *submitted = true;
+  return HPR_OK;
+}
+
+int solve_resident_end(Ctx* c, const ResidentJob& job, const hpr_results& done, hpr_results* out) {
+  hpr_results r = done;
   // times from the start of the eigenvalue estimate, as the host loop's
-  auto shift = [&](double t) { return t + S.power_time; };
+  auto shift = [&](double t) { return t + job.power_time; };
   r.time = shift(r.time);
   r.time_4 = shift(r.time_4);
   r.time_6 = shift(r.time_6);
-  r.power_time = S.power_time;
-  r.lambda_max_A = S.lamA;
-  r.lambda_max_Q = S.lamQ;
-  const double t_back = now_s();
+  r.power_time = job.power_time;
+  r.lambda_max_A = job.lamA;
+  r.lambda_max_Q = job.lamQ;
   if (out) {
     r.x = out->x;
     r.y = out->y;
@@ -627,11 +634,30 @@ int solve_resident(Ctx* c, const hpr_params* P, hpr_results* out, DQueue* q, dou
     *out = r;
     HPR_TRY(launch_unscale(c, out->x, out->y, out->z, out->w));
   }
-  if (phases) {
-    phases[2] = t_back - t_loop;
-    phases[3] = now_s() - t_back;
-  }
   return HPR_OK;
+}
+
+int solve_resident(Ctx* c, const hpr_params* P, hpr_results* out, DQueue* q, double* phases) {
+  ResidentJob job;
+  bool submitted = false;
+  HPR_TRY(solve_resident_begin(c, P, out, q, &job, &submitted, phases));
+  if (!submitted) return HPR_OK;
+  hpr_results r;
+  std::memset(&r, 0, sizeof(r));
+  int pause_us = 20;
+  double t_keep = now_s();
+  for (;;) {
+    bool done = false;
+    HPR_TRY(dqueue_poll(q, c, job.slot, &r, &done));
+    if (done) break;
+    std::this_thread::sleep_for(std::chrono::microseconds(pause_us));
+    pause_us = std::min(2 * pause_us, 500);
+    if (now_s() - t_keep > 2e-3) {
+      t_keep = now_s();
+      HPR_TRY(dqueue_keepalive(q) == HPR_OK ? HPR_OK : set_err(c, HPR_E_CUDA, "request loop launch failed"));
+    }
+  }
+  return solve_resident_end(c, job, r, out);
 }
 
 }  // namespace hpr
@@ -742,6 +768,11 @@ int hpr_create(int device, size_t budget, hpr_ctx** out) {
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
       uint64_t keep = ~0ull, reserved = 0, inuse = 0;
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      // a block freed on one context's stream is not handed to another
+      // context's stream behind an inserted wait on the first stream's work:
+      // concurrent contexts (the serving slots) would otherwise serialise
+      int no = 0;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
       if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
           cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &inuse) == cudaSuccess && reserved > inuse)
         fr += (size_t)(reserved - inuse);

@@ -68,6 +68,10 @@ struct DOut {
   int32_t error;  // HPR_OK or HPR_E_NUMERIC
   int32_t done;
   hpr_residuals last;
+  // seconds of the CTA in: iterations, residual checks, M-norms, sigma
+  // updates, restarts; and the number of residual checks
+  double t_iter, t_res, t_mnorm, t_sigma, t_restart;
+  int64_t checks;
 };
 
 struct DCtl {
@@ -111,13 +115,19 @@ __device__ void blk_map(int64_t n, F f) {
 // One engine pass over a matrix side: xin gathered, epilogue `e`, reduction
 // slots in d.red; with NRED > 0 the slots are then reduced in slot order.
 // The pass's arguments live in shared memory (one copy for the CTA, read
-// by every warp) rather than in each thread's local memory.
+// by every warp, copied by the CTA's threads word by word).  Each pass is
+// a function of its own, so its tile loop gets a register allocation of its
+// own instead of sharing one with the whole solve loop.
+static_assert(sizeof(EngineArgs) % 8 == 0, "EngineArgs copied in 8-byte words");
 template <class E>
-__device__ void blk_pass(const EngineArgs& base, const double* xin, E e, double* slots, WarpSmem& ws, BlkShared& sh,
-                         double* out) {
+__device__ __noinline__ void blk_pass(const EngineArgs& base, const double* xin, E e, double* slots, WarpSmem& ws,
+                                      BlkShared& sh, double* out) {
   __shared__ EngineArgs a;
+  constexpr int kWords = (int)(sizeof(EngineArgs) / 8);
+  if (threadIdx.x < kWords)
+    reinterpret_cast<uint64_t*>(&a)[threadIdx.x] = reinterpret_cast<const uint64_t*>(&base)[threadIdx.x];
+  __syncthreads();
   if (threadIdx.x == 0) {
-    a = base;
     a.xin = xin;
     a.xin32 = nullptr;
     a.red_slots = slots;
@@ -610,7 +620,12 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
   __shared__ int64_t s_iter, s_next, iter_4, iter_6;
   __shared__ double time_4, time_6;
   __shared__ int status, s_check, s_err;
+  __shared__ double tp[5];  // phase seconds (see DOut)
+  __shared__ int64_t n_checks;
   const int64_t ci = d.check_iter;
+  auto mark = [&](int k, double t0) {
+    if (threadIdx.x == 0) tp[k] += now_s() - t0;
+  };
   if (threadIdx.x == 0) {
     R.sigma = d.sigma0;
     R.flag = 0;
@@ -629,6 +644,8 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
     time_4 = time_6 = 0.0;
     status = -1;
     s_err = 0;
+    for (int k = 0; k < 5; ++k) tp[k] = 0.0;
+    n_checks = 0;
   }
   __syncthreads();
   while (true) {
@@ -639,7 +656,12 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
       s_check = (s_iter % ci == 0 || print_yes) ? 1 : 0;
     }
     __syncthreads();
-    if (s_check) blk_residuals(d, s_iter == 0, &rs, ws, sh);
+    if (s_check) {
+      const double t0 = now_s();
+      blk_residuals(d, s_iter == 0, &rs, ws, sh);
+      mark(1, t0);
+      if (threadIdx.x == 0) ++n_checks;
+    }
     if (threadIdx.x == 0) {
       const double kkt = rs.KKTx_and_gap_org_bar;
       if (kkt != kkt) s_err = HPR_E_NUMERIC;
@@ -651,6 +673,7 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
     __syncthreads();
     if (s_err) break;
     // ---- sigma update (update_sigma!, algorithm.jl:729-990)
+    const double t_sig = now_s();
     if (R.flag >= 1) {
       __shared__ double ta, tb, tc, td, s_sm;
       double a, b, cc, dd;
@@ -676,8 +699,11 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
       __syncthreads();
       if (s_sm != 0.0) blk_q_factors(d, R.sigma);
     }
+    mark(3, t_sig);
     if (R.flag > 0) {
+      const double t_rs = now_s();
       blk_restart(d, ws, sh);
+      mark(4, t_rs);
       if (threadIdx.x == 0) {
         R.last_gap = R.current_gap;
         R.save_gap = kInfD;
@@ -710,8 +736,12 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
     const int64_t next = s_next;
     int64_t iter = s_iter;
     if (R.flag > 0) {
+      double t0 = now_s();
       blk_iterate(d, 1, true, ws, sh);
+      mark(0, t0);
+      t0 = now_s();
       const double mn = blk_mnorm(d, R.sigma, ws, sh);
+      mark(2, t0);
       if (threadIdx.x == 0) {
         R.last_gap = cmin(mn, R.last_gap);
         if ((iter + 1) % ci == 0) R.current_gap = mn;
@@ -719,18 +749,26 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
       }
       iter += 1;
       if (iter < next) {
+        t0 = now_s();
         blk_iterate(d, next - iter, true, ws, sh);
+        mark(0, t0);
         if (threadIdx.x == 0) R.inner += next - iter;
         if (next % ci == 0) {
+          t0 = now_s();
           const double m2 = blk_mnorm(d, R.sigma, ws, sh);
+          mark(2, t0);
           if (threadIdx.x == 0) R.current_gap = m2;
         }
       }
     } else {
+      double t0 = now_s();
       blk_iterate(d, next - iter, true, ws, sh);
+      mark(0, t0);
       if (threadIdx.x == 0) R.inner += next - iter;
       if (next % ci == 0) {
+        t0 = now_s();
         const double m2 = blk_mnorm(d, R.sigma, ws, sh);
+        mark(2, t0);
         if (threadIdx.x == 0) R.current_gap = m2;
       }
     }
@@ -750,6 +788,12 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
     out->iter_6 = (iter_6 == 0 && time_6 == 0.0) ? s_iter : iter_6;
     out->sigma_final = R.sigma;
     out->last = rs;
+    out->t_iter = tp[0];
+    out->t_res = tp[1];
+    out->t_mnorm = tp[2];
+    out->t_sigma = tp[3];
+    out->t_restart = tp[4];
+    out->checks = n_checks;
   }
 }
 
@@ -766,7 +810,7 @@ __device__ __forceinline__ int ld_acquire_gpu(const int32_t* p) {
 // done in host memory.  The host copies each descriptor and then the new
 // published count into device memory; a CTA polls the count with a growing
 // pause (1 to 64 us) and exits after kIdleNs without a request.
-__global__ void __launch_bounds__(kDThreads, 2)
+__global__ void __launch_bounds__(kDThreads, 1)
     request_loop_kernel(const DSolve* __restrict__ reqs, DOut* outs, DCtl* ctl, int cap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem& ws = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
@@ -915,9 +959,9 @@ void dqueue_destroy(DQueue* q) {
 
 const char* dqueue_error(DQueue* q) { return q ? q->err.c_str() : ""; }
 
-// Build the request from the context (after solve_setup), publish it, wait
-// for its CTA and fill `out` (scalars; the solution stays on the context).
-int dqueue_solve(DQueue* q, Ctx* c, const hpr_params* P, double sigma0, hpr_results* out) {
+// Build the request from the context (after solve_setup) and publish it;
+// *slot_out identifies it for dqueue_poll.
+int dqueue_submit(DQueue* q, Ctx* c, const hpr_params* P, double sigma0, int* slot_out) {
   DSolve d = DSolve();
   auto args = [&](const DevCSR& M, const Plan& p, const int32_t* cs) {
     EngineArgs a = EngineArgs();
@@ -1023,20 +1067,24 @@ int dqueue_solve(DQueue* q, Ctx* c, const hpr_params* P, double sigma0, hpr_resu
       return set_err(c, HPR_E_CUDA, q->err);
     }
   }
-  // wait for the CTA; relaunch the loop if it went idle before taking it
+  *slot_out = slot;
+  return HPR_OK;
+}
+
+// Relaunch the request loop if it went idle while requests wait (the loop's
+// CTAs exit after kIdleNs without work); call it every few milliseconds
+// while requests are in flight.
+int dqueue_keepalive(DQueue* q) {
+  std::unique_lock<std::mutex> lk(q->mu);
+  return ensure_running(q);
+}
+
+// Non-blocking: when the request in `slot` is done, fill `out` (scalars; the
+// solution stays on the context), free the slot and set *done.
+int dqueue_poll(DQueue* q, Ctx* c, int slot, hpr_results* out, bool* done) {
   volatile DOut* o = q->h_outs + slot;
-  auto t_last = std::chrono::steady_clock::now();
-  int pause_us = 20;  // polls back off to 0.5 ms: many waiting slots cost little CPU
-  while (o->done == 0) {
-    std::this_thread::sleep_for(std::chrono::microseconds(pause_us));
-    pause_us = std::min(2 * pause_us, 500);
-    const auto now = std::chrono::steady_clock::now();
-    if (now - t_last > std::chrono::milliseconds(2)) {
-      t_last = now;
-      std::unique_lock<std::mutex> lk(q->mu);
-      if (ensure_running(q) != HPR_OK) return set_err(c, HPR_E_CUDA, q->err);
-    }
-  }
+  *done = false;
+  if (o->done == 0) return HPR_OK;
   std::atomic_thread_fence(std::memory_order_seq_cst);
   DOut r;
   std::memcpy(&r, (const void*)o, sizeof(DOut));
@@ -1044,6 +1092,7 @@ int dqueue_solve(DQueue* q, Ctx* c, const hpr_params* P, double sigma0, hpr_resu
     std::unique_lock<std::mutex> lk(q->mu);
     q->busy[slot] = 0;
   }
+  *done = true;
   if (r.error == HPR_E_NUMERIC)
     return set_err(c, HPR_E_NUMERIC, "NaN in the KKT residuals at iteration " + std::to_string(r.iter));
   out->iter = r.iter;
@@ -1060,7 +1109,34 @@ int dqueue_solve(DQueue* q, Ctx* c, const hpr_params* P, double sigma0, hpr_resu
   out->primal_obj = r.last.primal_obj_bar;
   out->gap = r.last.rel_gap_bar;
   c->sigma = r.sigma_final;
+  c->dloop[0] = r.t_iter;
+  c->dloop[1] = r.t_res;
+  c->dloop[2] = r.t_mnorm;
+  c->dloop[3] = r.t_sigma;
+  c->dloop[4] = r.t_restart;
+  c->dloop[5] = (double)r.checks;
   return HPR_OK;
+}
+
+// Publish and wait (polls back off to 0.5 ms, so many waiting threads cost
+// little CPU).
+int dqueue_solve(DQueue* q, Ctx* c, const hpr_params* P, double sigma0, hpr_results* out) {
+  int slot = -1;
+  HPR_TRY(dqueue_submit(q, c, P, sigma0, &slot));
+  int pause_us = 20;
+  auto t_last = std::chrono::steady_clock::now();
+  for (;;) {
+    bool done = false;
+    HPR_TRY(dqueue_poll(q, c, slot, out, &done));
+    if (done) return HPR_OK;
+    std::this_thread::sleep_for(std::chrono::microseconds(pause_us));
+    pause_us = std::min(2 * pause_us, 500);
+    const auto now = std::chrono::steady_clock::now();
+    if (now - t_last > std::chrono::milliseconds(2)) {
+      t_last = now;
+      if (dqueue_keepalive(q) != HPR_OK) return set_err(c, HPR_E_CUDA, q->err);
+    }
+  }
 }
 
 }  // namespace hpr

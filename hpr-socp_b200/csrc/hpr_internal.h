@@ -237,6 +237,9 @@ struct Ctx {
   void* q_user = nullptr;
   double q_lam = 0.0;
   double* qop_out = nullptr;
+  // the device-resident loop's split of its last solve: seconds in
+  // iterations, residual checks, M-norms, sigma updates, restarts; checks
+  double dloop[6] = {0, 0, 0, 0, 0, 0};
   double* vtmp_m = nullptr;
   float* g32_n = nullptr;  // FP32 copies of gathered vectors (x_hat/tempv, y)
   float* g32_m = nullptr;
@@ -333,12 +336,29 @@ bool dsolve_eligible(const Ctx* c, const hpr_params* P);
 // `cap` requests; null with *err set on failure
 DQueue* dqueue_create(int device, int ctas, int cap, std::string* err);
 void dqueue_destroy(DQueue* q);
-// hand a prepared context to the request loop and wait for its solve; fills
-// the scalars of `out` (not the vectors)
+// hand a prepared context to the request loop (non-blocking); *slot names it
+int dqueue_submit(DQueue* q, Ctx* c, const hpr_params* P, double sigma0, int* slot);
+// non-blocking completion check: when done, fills the scalars of `out` (not
+// the vectors) and frees the slot
+int dqueue_poll(DQueue* q, Ctx* c, int slot, hpr_results* out, bool* done);
+// relaunch the request loop if it went idle while requests wait
+int dqueue_keepalive(DQueue* q);
+// submit and wait
 int dqueue_solve(DQueue* q, Ctx* c, const hpr_params* P, double sigma0, hpr_results* out);
-// solve with the loop on the device when the problem fits (hpr_api.cu);
-// phases (may be null) receives the wall seconds of scaling, the eigenvalue
-// estimate, the loop and the unscaled read-back
+
+// A solve whose loop was handed to the request loop (hpr_api.cu).
+struct ResidentJob {
+  int slot = -1;
+  double power_time = 0.0, lamA = 0.0, lamQ = 0.0, t_loop = 0.0;
+};
+// setup, then either hand the loop to `q` (*submitted = true, finish with
+// solve_resident_end) or run the host loop to the end (*submitted = false);
+// phases (may be null): wall seconds of scaling, eigenvalue estimate, loop
+int solve_resident_begin(Ctx* c, const hpr_params* P, hpr_results* out, DQueue* q, ResidentJob* job,
+                         bool* submitted, double* phases = nullptr);
+// after dqueue_poll reported the job done: results and the unscaled solution
+int solve_resident_end(Ctx* c, const ResidentJob& job, const hpr_results& r, hpr_results* out);
+// solve with the loop on the device when the problem fits, waiting for it
 int solve_resident(Ctx* c, const hpr_params* P, hpr_results* out, DQueue* q, double* phases = nullptr);
 
 // auto-save of the current and best iterates (hpr_checkpoint.cu)

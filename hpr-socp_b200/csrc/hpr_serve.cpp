@@ -8,14 +8,17 @@
 // memory free up, and the kernels of all running solves overlap on the
 // device (small problems launch only the CTAs their tiles need).  Each
 // request carries its own parameters, so each retires at its own tolerance.
-// A request is uploaded, scaled and its eigenvalues estimated on the slot's
-// private context.  When the problem fits one CTA (hpr_dsolve.cu), its whole
-// solve loop then runs inside the device-resident request loop: one
-// persistent kernel whose CTAs each solve one request at a time, so the
-// loops of many requests run in one launch with no host round trip per
-// residual check.  Larger problems run the host-driven loop of hpr_solve.
-// Either way a request's result does not depend on the other requests: the
-// same request gives the same bits alone and in the mix.
+// A slot thread takes a request and a free solver context (the server keeps
+// four per slot), uploads the request, scales it and estimates its
+// eigenvalues.  When the problem fits one CTA (hpr_dsolve.cu), the thread
+// hands its whole solve loop to the device-resident request loop (one
+// persistent kernel whose CTAs each solve one request at a time, with no
+// host round trip per residual check) and goes on to the next request; a
+// finisher thread reads back the solutions of the requests the loop
+// completes and frees their contexts.  Larger problems run the host-driven
+// loop of hpr_solve on the slot thread.  Either way a request's result does
+// not depend on the other requests: the same request gives the same bits
+// alone and in the mix.
 //
 // The reference solves one model per `optimize` call (src/algorithm.jl:
 // 2538-2581) and its dataset runner loops over files one at a time
@@ -38,6 +41,10 @@
 #include <cuda_runtime.h>
 
 #include "hpr_internal.h"
+
+#ifndef HPR_SERVE_LOOP_SM_DIV
+#define HPR_SERVE_LOOP_SM_DIV 3  // the request loop takes at most SMs / this many CTAs
+#endif
 
 namespace {
 
@@ -140,38 +147,85 @@ size_t estimate_bytes(const hpr_problem& p) {
 
 }  // namespace
 
+// A request whose solve loop is in the device-resident request loop.
+struct InFlight {
+  Request r;
+  hpr_ctx* ctx = nullptr;
+  hpr::ResidentJob job;
+  Finished f;
+  double ph[6] = {0, 0, 0, 0, 0, 0};
+};
+
 struct hpr_server {
   int device = 0;
   size_t budget = 0, reserved = 0;
   std::mutex mu;
-  std::condition_variable cv_work, cv_done;
+  std::condition_variable cv_work, cv_done, cv_flight;
   std::deque<Request> queue;
   std::map<int64_t, Finished> done;
   std::set<int64_t> live;  // submitted and not yet consumed by a poll
   std::vector<std::thread> workers;
+  std::thread finisher;
+  std::vector<hpr_ctx*> ctx_all, ctx_free;  // solver contexts; the free ones hold no request
+  std::deque<InFlight> inflight;            // requests in the device loop
   int64_t next_ticket = 1;
   int64_t running = 0;
+  int workers_alive = 0;
   bool stop = false;
   std::string err;
   hpr::DQueue* dq = nullptr;  // device-resident request loop (null: host loops only)
   int resident = 1;
-  // wall seconds summed over finished requests: queue wait, upload, scaling,
-  // eigenvalue estimate, solve loop, unscaled read-back
-  double phase_sum[6] = {0, 0, 0, 0, 0, 0};
+  // summed over finished requests: wall seconds of queue wait, upload,
+  // scaling, eigenvalue estimate, solve loop, unscaled read-back; then the
+  // device-resident loop's seconds in iterations, residual checks, M-norms,
+  // sigma updates, restarts, and its residual-check count
+  double phase_sum[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   int64_t phase_count = 0;
 
-  void worker(hpr_ctx* ctx) {
+  // a request is over: record it and free its context and memory
+  void complete(Request& r, Finished&& f, hpr_ctx* ctx, const double* ph) {
+    f.res.x = f.res.y = f.res.z = f.res.w = nullptr;
+    f.latency = now_s() - r.t_submit;
+    r.prob.reset();
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      reserved -= r.est;
+      --running;
+      done[r.ticket] = std::move(f);
+      for (int k = 0; k < 6; ++k) phase_sum[k] += ph[k];
+      for (int k = 0; k < 6; ++k) phase_sum[6 + k] += ctx->c.dloop[k];
+      for (int k = 0; k < 6; ++k) ctx->c.dloop[k] = 0.0;
+      ++phase_count;
+      ctx_free.push_back(ctx);
+    }
+    cv_done.notify_all();
+    cv_work.notify_all();
+  }
+
+  // A slot thread: takes the head of the queue once its memory fits and a
+  // context is free, uploads it, scales it and estimates its eigenvalues,
+  // then either hands the solve loop to the device (and goes on to the next
+  // request) or runs the host loop to the end.
+  void worker() {
+    cudaSetDevice(device);
     for (;;) {
       Request r;
+      hpr_ctx* ctx = nullptr;
       {
         std::unique_lock<std::mutex> lk(mu);
-        // admission: the head of the queue enters once its memory fits
-        cv_work.wait(lk, [&] { return stop || (!queue.empty() && reserved + queue.front().est <= budget); });
-        if (stop) break;
+        cv_work.wait(lk, [&] {
+          return stop || (!queue.empty() && reserved + queue.front().est <= budget && !ctx_free.empty());
+        });
+        if (stop) {
+          --workers_alive;
+          break;
+        }
         r = std::move(queue.front());
         queue.pop_front();
         reserved += r.est;
         ++running;
+        ctx = ctx_free.back();
+        ctx_free.pop_back();
       }
       Finished f;
       const int64_t n = r.prob->p.n, m = r.prob->p.m;
@@ -191,26 +245,94 @@ struct hpr_server {
       ph[0] = t_start - r.t_submit;
       f.rc = hpr_upload(ctx, &r.prob->p);
       ph[1] = now_s() - t_start;
-      if (f.rc == HPR_OK) {
-        cudaSetDevice(device);
-        f.rc = hpr::solve_resident(&ctx->c, &r.params, &f.res, resident ? dq : nullptr, ph + 2);
-      }
+      hpr::ResidentJob job;
+      bool submitted = false;
+      if (f.rc == HPR_OK)
+        f.rc = hpr::solve_resident_begin(&ctx->c, &r.params, &f.res, resident ? dq : nullptr, &job, &submitted,
+                                         ph + 2);
       if (f.rc != HPR_OK) f.err = hpr_last_error(ctx);
-      f.res.x = f.res.y = f.res.z = f.res.w = nullptr;
-      f.latency = now_s() - r.t_submit;
-      r.prob.reset();
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        reserved -= r.est;
-        --running;
-        done[r.ticket] = std::move(f);
-        for (int k = 0; k < 6; ++k) phase_sum[k] += ph[k];
-        ++phase_count;
+      if (f.rc == HPR_OK && submitted) {
+        InFlight fl;
+        fl.r = std::move(r);
+        fl.ctx = ctx;
+        fl.job = job;
+        fl.f = std::move(f);
+        std::copy(ph, ph + 6, fl.ph);
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          inflight.push_back(std::move(fl));
+        }
+        cv_flight.notify_one();
+        continue;
       }
-      cv_done.notify_all();
-      cv_work.notify_all();
+      complete(r, std::move(f), ctx, ph);
     }
-    hpr_destroy(ctx);
+  }
+
+  // Completes the requests of the device loop: polls their done flags,
+  // reads back the unscaled solutions and frees their contexts.  It keeps
+  // the request loop running while requests wait and drains them at stop.
+  void finish_loop() {
+    cudaSetDevice(device);
+    double t_keep = 0.0;
+    int pause_us = 20;
+    for (;;) {
+      std::vector<InFlight> ready;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        if (inflight.empty()) {
+          // at stop, the loop ends once no slot thread can hand over more
+          if (stop && workers_alive == 0) break;
+          cv_flight.wait_for(lk, std::chrono::milliseconds(5));
+          continue;
+        }
+        for (auto it = inflight.begin(); it != inflight.end();) {
+          bool fin = false;
+          hpr_results r{};
+          const int rc = hpr::dqueue_poll(dq, &it->ctx->c, it->job.slot, &r, &fin);
+          if (fin || rc != HPR_OK) {
+            InFlight fl = std::move(*it);
+            it = inflight.erase(it);
+            if (rc != HPR_OK) {
+              fl.f.rc = rc;
+              fl.f.err = hpr_last_error(fl.ctx);
+            } else {
+              // the done result's scalars travel in f.res until the read-back
+              double *x = fl.f.res.x, *y = fl.f.res.y, *z = fl.f.res.z, *w = fl.f.res.w;
+              fl.f.res = r;
+              fl.f.res.x = x;
+              fl.f.res.y = y;
+              fl.f.res.z = z;
+              fl.f.res.w = w;
+            }
+            ready.push_back(std::move(fl));
+          } else {
+            ++it;
+          }
+        }
+      }
+      if (now_s() - t_keep > 2e-3) {
+        t_keep = now_s();
+        hpr::dqueue_keepalive(dq);
+      }
+      if (ready.empty()) {
+        std::this_thread::sleep_for(std::chrono::microseconds(pause_us));
+        pause_us = std::min(2 * pause_us, 200);
+        continue;
+      }
+      pause_us = 20;
+      for (InFlight& fl : ready) {
+        const double t_back = now_s();
+        fl.ph[4] = t_back - fl.job.t_loop;
+        if (fl.f.rc == HPR_OK) {
+          const hpr_results r = fl.f.res;
+          fl.f.rc = hpr::solve_resident_end(&fl.ctx->c, fl.job, r, &fl.f.res);
+          if (fl.f.rc != HPR_OK) fl.f.err = hpr_last_error(fl.ctx);
+        }
+        fl.ph[5] = now_s() - t_back;
+        complete(fl.r, std::move(fl.f), fl.ctx, fl.ph);
+      }
+    }
   }
 };
 
@@ -224,8 +346,16 @@ int hpr_serve_create(int device, int slots, size_t hbm_budget, hpr_server** out)
   // it is set before the process creates its CUDA context (an existing
   // setting is kept).
   setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
+  // Many slot threads wait on the device at once: when the server creates
+  // the process's CUDA context, its waits block instead of spinning, so the
+  // waiting threads leave the host cores to the threads preparing requests.
+  // (An existing context keeps its own mode; the call then fails harmlessly.)
+  if (cudaInitDevice(device, cudaDeviceScheduleBlockingSync, 0) != cudaSuccess) (void)cudaGetLastError();
+  // up to four requests per slot thread can be in the device loop at once,
+  // each on a context of its own
+  const int nctx = 4 * slots;
   std::vector<hpr_ctx*> ctxs;
-  for (int i = 0; i < slots; ++i) {
+  for (int i = 0; i < nctx; ++i) {
     hpr_ctx* c = nullptr;
     int rc = hpr_create(device, 0, &c);
     if (rc != HPR_OK) {
@@ -248,13 +378,24 @@ int hpr_serve_create(int device, int slots, size_t hbm_budget, hpr_server** out)
   }
   s->budget = hbm_budget;
   std::string qerr;
-  s->dq = hpr::dqueue_create(device, 0, 4096, &qerr);
+  // one CTA of the request loop per context that can be in it, and at most
+  // a third of the SMs (a loop CTA takes a whole SM's registers): the other
+  // SMs stay free for the upload, scaling and eigenvalue kernels of the
+  // requests being set up and for the multi-CTA engine of the requests too
+  // large for one CTA
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  s->dq = hpr::dqueue_create(device, std::max(1, std::min(nctx, sms / HPR_SERVE_LOOP_SM_DIV)), 4096, &qerr);
   if (!s->dq) {
     for (hpr_ctx* d : ctxs) hpr_destroy(d);
     delete s;
     return HPR_E_CUDA;
   }
-  for (hpr_ctx* c : ctxs) s->workers.emplace_back([s, c] { s->worker(c); });
+  s->ctx_all = ctxs;
+  s->ctx_free = ctxs;
+  s->workers_alive = slots;
+  for (int i = 0; i < slots; ++i) s->workers.emplace_back([s] { s->worker(); });
+  s->finisher = std::thread([s] { s->finish_loop(); });
   *out = s;
   return HPR_OK;
 }
@@ -356,7 +497,7 @@ int hpr_serve_stats(hpr_server* s, int64_t* queued, int64_t* running, size_t* re
 int hpr_serve_phase_times(hpr_server* s, double* seconds, int64_t* requests) {
   if (!s || !seconds) return HPR_E_BAD_INPUT;
   std::lock_guard<std::mutex> lk(s->mu);
-  for (int k = 0; k < 6; ++k) seconds[k] = s->phase_sum[k];
+  for (int k = 0; k < 12; ++k) seconds[k] = s->phase_sum[k];
   if (requests) *requests = s->phase_count;
   return HPR_OK;
 }
@@ -371,8 +512,12 @@ int hpr_serve_destroy(hpr_server* s) {
   }
   s->cv_work.notify_all();
   s->cv_done.notify_all();
+  s->cv_flight.notify_all();
   for (std::thread& t : s->workers) t.join();
+  // requests still in the device loop finish there first
+  if (s->finisher.joinable()) s->finisher.join();
   hpr::dqueue_destroy(s->dq);
+  for (hpr_ctx* c : s->ctx_all) hpr_destroy(c);
   delete s;
   return HPR_OK;
 }

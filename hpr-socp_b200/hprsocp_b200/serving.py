@@ -65,12 +65,16 @@ class Server:
         return {"queued": q.value, "running": run.value, "reserved_bytes": res.value}
 
     def phase_times(self):
-        """Mean wall seconds per finished request: queue wait, upload,
-        scaling, eigenvalue estimate, solve loop, read-back."""
-        sec = (C.c_double * 6)()
+        """Mean per finished request: wall seconds of queue wait, upload,
+        scaling, eigenvalue estimate, solve loop, read-back; the device
+        loop's seconds in iterations, residual checks, M-norms, sigma
+        updates, restarts, and its residual checks."""
+        sec = (C.c_double * 12)()
         n = C.c_int64()
         self.lib.hpr_serve_phase_times(self.h, sec, C.byref(n))
-        names = ("queue_wait", "upload", "scaling", "power_iteration", "solve_loop", "readback")
+        names = ("queue_wait", "upload", "scaling", "power_iteration", "solve_loop", "readback",
+                 "device_iterations", "device_residual_checks", "device_mnorm", "device_sigma", "device_restart",
+                 "device_checks")
         return {k: (sec[i] / n.value if n.value else 0.0) for i, k in enumerate(names)}
 
     def close(self):

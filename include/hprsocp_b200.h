@@ -462,9 +462,11 @@ int hpr_serve_poll(hpr_server* srv, int64_t ticket, int wait_ms,
 int hpr_serve_stats(hpr_server* srv, int64_t* queued, int64_t* running,
                     size_t* reserved_bytes);
 
-/* Wall seconds spent by the finished requests, summed, in seconds[0..5]:
- * queue wait, upload, scaling, eigenvalue estimate, solve loop, unscaled
- * read-back; *requests = how many requests they cover.                     */
+/* Time spent by the finished requests, summed: seconds[0..5] wall seconds
+ * of queue wait, upload, scaling, eigenvalue estimate, solve loop, unscaled
+ * read-back; seconds[6..10] the device-resident loop's seconds in
+ * iterations, residual checks, M-norms, sigma updates and restarts;
+ * seconds[11] its residual checks.  *requests = how many requests.        */
 int hpr_serve_phase_times(hpr_server* srv, double* seconds, int64_t* requests);
 const char* hpr_serve_last_error(hpr_server* srv);
 
