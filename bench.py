@@ -213,7 +213,7 @@ def run_reference(args, model, budget_s=150.0):
     print(json.dumps(line))
 
 
-def serving_measure(requests, slots=32, rate=0.0, baseline=60, resident=True, seed=11):
+def serving_measure(requests, slots=32, rate=0.0, baseline=60, resident=False, seed=11):
     """Serving stream: small SOCPs (n lognormal, median 400) with per-request
     tolerances 1e-4 / 1e-6 through the continuous-batching server, against
     the same requests solved one at a time with hpr_optimize."""
@@ -282,7 +282,7 @@ def serving_measure(requests, slots=32, rate=0.0, baseline=60, resident=True, se
 
 
 def run_serving(args):
-    d = serving_measure(args.requests, args.slots, args.rate, args.baseline, resident=not args.host_loop)
+    d = serving_measure(args.requests, args.slots, args.rate, args.baseline, resident=args.resident)
     line = {"metric": "solves/s", "value": d["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
             "steps": d["requests"], "warmup": 2, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded serving stream, seed 11)",
@@ -376,7 +376,8 @@ def main():
     ap.add_argument("--slots", type=int, default=32, help="serve: concurrent solver slots")
     ap.add_argument("--rate", type=float, default=0.0, help="serve: Poisson arrivals/s (0 = saturation)")
     ap.add_argument("--baseline", type=int, default=60, help="serve: requests solved one at a time")
-    ap.add_argument("--host-loop", action="store_true", help="serve: keep every solve loop on the host")
+    ap.add_argument("--resident", action="store_true",
+                    help="serve: small problems' solve loops in the device-resident request loop")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -482,7 +483,7 @@ def main():
     serving = None
     if not args.no_serve:
         # a fixed 200-request sample of the serving stream (config 4) through
-        # the device-resident request loop, against one-at-a-time solves
+        # the server, against one-at-a-time solves
         serving = serving_measure(200, slots=32, baseline=30)
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "engine_config1_dram_bytes.txt")

@@ -115,24 +115,40 @@ __device__ void blk_map(int64_t n, F f) {
 // One engine pass over a matrix side: xin gathered, epilogue `e`, reduction
 // slots in d.red; with NRED > 0 the slots are then reduced in slot order.
 // The pass's arguments live in shared memory (one copy for the CTA, read
-// by every warp, copied by the CTA's threads word by word).  Each pass is
-// a function of its own, so its tile loop gets a register allocation of its
-// own instead of sharing one with the whole solve loop.
+// by every warp).  Each pass is a function of its own, so its tile loop
+// gets a register allocation of its own instead of sharing one with the
+// whole solve loop.
 static_assert(sizeof(EngineArgs) % 8 == 0, "EngineArgs copied in 8-byte words");
-template <class E>
-__device__ __noinline__ void blk_pass(const EngineArgs& base, const double* xin, E e, double* slots, WarpSmem& ws,
-                                      BlkShared& sh, double* out) {
-  __shared__ EngineArgs a;
+
+// dst (shared) = base with xin and the reduction slots set; all threads call
+__device__ void blk_args(EngineArgs& dst, const EngineArgs& base, const double* xin, double* slots) {
   constexpr int kWords = (int)(sizeof(EngineArgs) / 8);
   if (threadIdx.x < kWords)
-    reinterpret_cast<uint64_t*>(&a)[threadIdx.x] = reinterpret_cast<const uint64_t*>(&base)[threadIdx.x];
+    reinterpret_cast<uint64_t*>(&dst)[threadIdx.x] = reinterpret_cast<const uint64_t*>(&base)[threadIdx.x];
   __syncthreads();
   if (threadIdx.x == 0) {
-    a.xin = xin;
-    a.xin32 = nullptr;
-    a.red_slots = slots;
+    dst.xin = xin;
+    dst.xin32 = nullptr;
+    dst.red_slots = slots;
   }
   __syncthreads();
+}
+
+// One pass over prepared (shared-memory) arguments.
+template <class E>
+__device__ __noinline__ void blk_pass_args(const EngineArgs& a, E e, WarpSmem& ws, BlkShared& sh, double* out);
+
+template <class E>
+__device__ void blk_pass(const EngineArgs& base, const double* xin, E e, double* slots, WarpSmem& ws, BlkShared& sh,
+                         double* out) {
+  __shared__ EngineArgs a;
+  blk_args(a, base, xin, slots);
+  blk_pass_args(a, e, ws, sh, out);
+}
+
+template <class E>
+__device__ __noinline__ void blk_pass_args(const EngineArgs& a, E e, WarpSmem& ws, BlkShared& sh, double* out) {
+  double* slots = a.red_slots;
   e.setup(a.st);
   for (int t = threadIdx.x >> 5; t < a.pv.ntasks; t += kWarpsPerCta)
     process_warp_tile<E, HPR_PREC_FP64, true, kFusedChunk>(a, e, t, ws);
@@ -164,22 +180,40 @@ __device__ void blk_qmap(const DSolve& d, const double* v, double* out, WarpSmem
   blk_pass(d.aq, v, plain_epi(out), nullptr, ws, sh, nullptr);
 }
 
+// The iteration passes' arguments, prepared once per request.
+struct IterArgs {
+  EngineArgs x, y, qw, qwb;  // no Q: x (A', y), y (A, x_hat); Q: qw, qwb, y (A, tempv), x (A', y_bar)
+};
+
+__device__ void blk_iter_args(const DSolve& d, IterArgs& ia) {
+  if (!d.has_q) {
+    blk_args(ia.x, d.ax, d.y, nullptr);
+    blk_args(ia.y, d.ay, d.x_hat, nullptr);
+  } else {
+    blk_args(ia.qw, d.aq, d.w, nullptr);
+    blk_args(ia.qwb, d.aq, d.w_bar, nullptr);
+    blk_args(ia.y, d.ay, d.tempv, nullptr);
+    blk_args(ia.x, d.ax, d.y_bar, nullptr);
+  }
+}
+
 // k HPR iterations, the last one full when full_last (the single-CTA
 // kernel's loop; thread 0 advances the Halpern counter).
-__device__ void blk_iterate(const DSolve& d, int64_t k, bool full_last, WarpSmem& ws, BlkShared& sh) {
+__device__ void blk_iterate(const DSolve& d, const IterArgs& ia, int64_t k, bool full_last, WarpSmem& ws,
+                            BlkShared& sh) {
   for (int64_t it = 0; it < k; ++it) {
     const bool last = full_last && it + 1 == k;
     const IterEpis& E = last ? d.full : d.part;
     if (!d.has_q) {
-      blk_pass(d.ax, d.y, E.ex, nullptr, ws, sh, nullptr);
-      if (d.m > 0) blk_pass(d.ay, d.x_hat, E.ey, nullptr, ws, sh, nullptr);
+      blk_pass_args(ia.x, E.ex, ws, sh, nullptr);
+      if (d.m > 0) blk_pass_args(ia.y, E.ey, ws, sh, nullptr);
     } else {
-      blk_pass(d.aq, d.w, E.eq, nullptr, ws, sh, nullptr);
+      blk_pass_args(ia.qw, E.eq, ws, sh, nullptr);
       if (d.m > 0) {
-        blk_pass(d.aq, d.w_bar, E.et, nullptr, ws, sh, nullptr);
-        blk_pass(d.ay, d.tempv, E.ey, nullptr, ws, sh, nullptr);
+        blk_pass_args(ia.qwb, E.et, ws, sh, nullptr);
+        blk_pass_args(ia.y, E.ey, ws, sh, nullptr);
       }
-      blk_pass(d.ax, d.y_bar, E.e2, nullptr, ws, sh, nullptr);
+      blk_pass_args(ia.x, E.e2, ws, sh, nullptr);
     }
     if (threadIdx.x == 0) d.st->inner = d.st->inner + 1;
     __syncthreads();
@@ -621,6 +655,8 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
   __shared__ double time_4, time_6;
   __shared__ int status, s_check, s_err;
   __shared__ double tp[5];  // phase seconds (see DOut)
+  __shared__ IterArgs ia;
+  blk_iter_args(d, ia);
   __shared__ int64_t n_checks;
   const int64_t ci = d.check_iter;
   auto mark = [&](int k, double t0) {
@@ -737,7 +773,7 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
     int64_t iter = s_iter;
     if (R.flag > 0) {
       double t0 = now_s();
-      blk_iterate(d, 1, true, ws, sh);
+      blk_iterate(d, ia, 1, true, ws, sh);
       mark(0, t0);
       t0 = now_s();
       const double mn = blk_mnorm(d, R.sigma, ws, sh);
@@ -750,7 +786,7 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
       iter += 1;
       if (iter < next) {
         t0 = now_s();
-        blk_iterate(d, next - iter, true, ws, sh);
+        blk_iterate(d, ia, next - iter, true, ws, sh);
         mark(0, t0);
         if (threadIdx.x == 0) R.inner += next - iter;
         if (next % ci == 0) {
@@ -762,7 +798,7 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
       }
     } else {
       double t0 = now_s();
-      blk_iterate(d, next - iter, true, ws, sh);
+      blk_iterate(d, ia, next - iter, true, ws, sh);
       mark(0, t0);
       if (threadIdx.x == 0) R.inner += next - iter;
       if (next % ci == 0) {

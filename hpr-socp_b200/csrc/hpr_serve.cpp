@@ -174,7 +174,7 @@ struct hpr_server {
   bool stop = false;
   std::string err;
   hpr::DQueue* dq = nullptr;  // device-resident request loop (null: host loops only)
-  int resident = 1;
+  int resident = 0;           // hpr_serve_set_resident
   // summed over finished requests: wall seconds of queue wait, upload,
   // scaling, eigenvalue estimate, solve loop, unscaled read-back; then the
   // device-resident loop's seconds in iterations, residual checks, M-norms,

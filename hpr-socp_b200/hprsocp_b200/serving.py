@@ -16,7 +16,7 @@ class Server:
     """`slots` solver contexts on one device; requests are admitted while
     their estimated device memory fits `hbm_budget` bytes (0 = 90% of free)."""
 
-    def __init__(self, slots: int = 16, device: int = 0, hbm_budget: int = 0, resident: bool = True):
+    def __init__(self, slots: int = 16, device: int = 0, hbm_budget: int = 0, resident: bool = False):
         self.lib = _abi.load_library()
         h = C.c_void_p()
         rc = self.lib.hpr_serve_create(device, slots, hbm_budget, C.byref(h))
@@ -25,7 +25,8 @@ class Server:
         self.h = h
         self._shapes = {}
         # resident: small problems run their whole solve loop in the
-        # device-resident request loop; False keeps every loop on the host
+        # device-resident request loop; False (default) keeps every loop on
+        # the host
         self.lib.hpr_serve_set_resident(self.h, 1 if resident else 0)
 
     def _err(self, rc):

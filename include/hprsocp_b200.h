@@ -427,21 +427,25 @@ int hpr_iteration_bytes(hpr_ctx* ctx, double* bytes_per_iter);
 /* ------------------------------------------------------------------------ */
 typedef struct hpr_server hpr_server;
 
-/* `slots` solver contexts (one stream and host thread each) on `device`;
- * requests are admitted while their estimated device memory fits
- * `hbm_budget` bytes (0 = 90% of the device's free memory).  A slot
- * uploads, scales and estimates the eigenvalues of its request; a problem
- * small enough for one CTA (every matrix side within the single-CTA tile
- * limit, FP64, no operator Q, no auto-save) is then solved by the
- * device-resident request loop: a persistent kernel, one CTA per solve,
- * running the whole HPR loop (iterations, residual checks, restarts, sigma
- * updates, termination) on the device.  Other requests run the host loop
- * of hpr_solve.                                                            */
+/* `slots` host threads on `device`, each taking requests from the queue
+ * while their estimated device memory fits `hbm_budget` bytes (0 = 90% of
+ * the device's free memory) and a solver context is free (four per slot).
+ * A slot uploads, scales and estimates the eigenvalues of its request on
+ * its context, then runs the solve loop of hpr_solve (the default), or,
+ * with hpr_serve_set_resident(srv, 1), hands a problem small enough for one
+ * CTA to the device-resident request loop and goes on to the next request. */
 int hpr_serve_create(int device, int slots, size_t hbm_budget,
                      hpr_server** out);
 
-/* 1 (default): eligible requests use the device-resident request loop;
- * 0: every request runs the host loop of hpr_solve (for comparisons).     */
+/* 1: problems small enough for one CTA (every matrix side within the
+ * single-CTA tile limit, FP64, no operator Q, no auto-save) are solved by
+ * the device-resident request loop, a persistent kernel with one CTA per
+ * solve running the whole HPR loop (iterations, residual checks, restarts,
+ * sigma updates, termination) on the device; a finisher thread reads the
+ * results back.  0 (default): every request runs the host loop.  The
+ * device loop takes as long per iteration as the single-CTA kernel of the
+ * host loop and measured lower throughput on the serving stream, so it is
+ * off by default.                                                          */
 int hpr_serve_set_resident(hpr_server* srv, int on);
 
 /* Queue one problem with its own parameters (tolerance, limits, precision);

@@ -19,16 +19,18 @@ def _params(tol):
     return HPRSOCP_parameters(verbose=False, stoptol=tol, max_iter=200000)
 
 
-def test_each_result_is_the_same_alone_and_in_the_mix(stream):
+@pytest.mark.parametrize("resident", [False, True])
+def test_each_result_is_the_same_alone_and_in_the_mix(stream, resident):
     """A request solved alone (a one-slot server, nothing else on the
     device) and the same request among 40 submitted at once to 16 slots give
-    the same bits: each small problem's loop runs in its own CTA of the
-    device-resident request loop, every reduction in a fixed order."""
+    the same bits, with the solve loops on the host or, for the problems
+    small enough, in the device-resident request loop (one CTA per solve):
+    every reduction has a fixed order."""
     alone = []
-    with Server(slots=1) as srv:
+    with Server(slots=1, resident=resident) as srv:
         for model, tol, _ in stream:
             alone.append(srv.poll(srv.submit(model, _params(tol)))[0])
-    with Server(slots=16) as srv:
+    with Server(slots=16, resident=resident) as srv:
         tickets = [srv.submit(model, _params(tol)) for model, tol, _ in stream]
         mixed = [srv.poll(t)[0] for t in tickets]
     for (model, tol, _), a, b in zip(stream, alone, mixed):
@@ -41,16 +43,17 @@ def test_each_result_is_the_same_alone_and_in_the_mix(stream):
 def test_device_loop_agrees_with_the_host_loop(stream):
     """The device-resident loop runs the host loop's logic with its
     reductions summed in another fixed order: each request reaches the same
-    status at its tolerance with the objective within 1e-6 and the iteration
-    count within one check interval.  With the resident loop switched off,
-    a server solve is hpr_solve on a private context, bit for bit."""
+    status at its tolerance with the objective within 10 x tol and the
+    iteration count within one check interval.  With the loops on the host
+    (the default), a server solve is hpr_solve on a private context, bit for
+    bit."""
     host = []
     for model, tol, _ in stream:
         with Context(model) as ctx:
             host.append(ctx.solve(_params(tol)))
-    with Server(slots=16) as srv:
+    with Server(slots=16, resident=True) as srv:
         dev = [srv.poll(t)[0] for t in [srv.submit(m, _params(tol)) for m, tol, _ in stream]]
-    with Server(slots=16, resident=False) as srv:
+    with Server(slots=16) as srv:
         off = [srv.poll(t)[0] for t in [srv.submit(m, _params(tol)) for m, tol, _ in stream]]
     for (model, tol, _), h, d, o in zip(stream, host, dev, off):
         assert h.status == d.status == "OPTIMAL" and d.residuals <= tol
