@@ -223,7 +223,7 @@ def serving_measure(requests, slots=32, rate=0.0, baseline=60, resident=False, s
     import numpy as np
     from hprsocp_b200 import HPRSOCP_parameters, _abi, instances
     from hprsocp_b200.serving import Server
-    stream = instances.serving_stream(seed, requests, rate=rate)
+    stream = instances.serving_stream(seed, requests, rate=rate, procs=os.cpu_count() or 1)
     params = [HPRSOCP_parameters(verbose=False, stoptol=tol, max_iter=200000) for _, tol, _ in stream]
     lib = _abi.load_library()
     # the server: requests submitted at their arrival times (all at t = 0 at

@@ -141,7 +141,8 @@ __device__ __noinline__ void blk_pass_args(const EngineArgs& a, E e, WarpSmem& w
 template <class E>
 __device__ void blk_pass(const EngineArgs& base, const double* xin, E e, double* slots, WarpSmem& ws, BlkShared& sh,
                          double* out) {
-  __shared__ EngineArgs a;
+  __shared__ __align__(16) unsigned char a_raw[sizeof(EngineArgs)];
+  EngineArgs& a = *reinterpret_cast<EngineArgs*>(a_raw);
   blk_args(a, base, xin, slots);
   blk_pass_args(a, e, ws, sh, out);
 }
@@ -655,7 +656,9 @@ __device__ void dsolve_run(const DSolve& d, DOut* out, double t_start, WarpSmem&
   __shared__ double time_4, time_6;
   __shared__ int status, s_check, s_err;
   __shared__ double tp[5];  // phase seconds (see DOut)
-  __shared__ IterArgs ia;
+  // (raw storage: shared variables are not constructed)
+  __shared__ __align__(16) unsigned char ia_raw[sizeof(IterArgs)];
+  IterArgs& ia = *reinterpret_cast<IterArgs*>(ia_raw);
   blk_iter_args(d, ia);
   __shared__ int64_t n_checks;
   const int64_t ci = d.check_iter;

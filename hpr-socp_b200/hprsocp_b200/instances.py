@@ -237,17 +237,24 @@ def small_socp(seed: int, n: int = None, diag_q: bool = None) -> SOCPModel:
     return model
 
 
-def serving_stream(seed: int, count: int, rate: float = 0.0):
+def serving_stream(seed: int, count: int, rate: float = 0.0, procs: int = 0):
     """The serving workload: `count` small SOCPs (small_socp) with a per-request
     tolerance of 1e-4 or 1e-6 (50/50) and Poisson arrival times at `rate`
     requests/s (rate <= 0: everything arrives at t = 0, i.e. saturation).
-    Returns a list of (model, stoptol, arrival_s)."""
+    Returns a list of (model, stoptol, arrival_s).  procs > 1 builds the
+    instances in that many worker processes (same instances)."""
     rng = np.random.default_rng(seed)
-    out = []
+    specs = []
     t = 0.0
     for k in range(count):
         tol = 1e-4 if rng.integers(0, 2) == 0 else 1e-6
         if rate > 0:
             t += rng.exponential(1.0 / rate)
-        out.append((small_socp(int(rng.integers(0, 2**31 - 1))), tol, t))
-    return out
+        specs.append((int(rng.integers(0, 2**31 - 1)), tol, t))
+    if procs > 1 and count > 64:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(procs) as pool:
+            models = pool.map(small_socp, [sd for sd, _, _ in specs], chunksize=64)
+    else:
+        models = [small_socp(sd) for sd, _, _ in specs]
+    return [(m, tol, t) for m, (_, tol, t) in zip(models, specs)]
