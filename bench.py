@@ -471,6 +471,12 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
+    serving = None
+    if not args.no_serve:
+        # a fixed 200-request sample of the serving stream (config 4) through
+        # the server, against one-at-a-time solves (before the CPU baseline,
+        # whose host threads would compete with the server's)
+        serving = serving_measure(200, slots=32, baseline=30)
     cpu = None
     if not args.no_cpu:
         iters = 3
@@ -480,11 +486,6 @@ def main():
                "one_thread": {"value": cpu_iteration_rate(model, iters=1, threads=1), "unit": "iter/s",
                               "cores": 1, "sample": "1 HPR iteration on one thread (the reference's CPU "
                                                     "path is single-threaded)"}}
-    serving = None
-    if not args.no_serve:
-        # a fixed 200-request sample of the serving stream (config 4) through
-        # the server, against one-at-a-time solves
-        serving = serving_measure(200, slots=32, baseline=30)
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "engine_config1_dram_bytes.txt")
     if os.path.exists(tfile):

@@ -95,7 +95,7 @@ void free_all(Ctx* c) {
                    &c->last_w, &c->dw,     &c->Qw,     &c->dQw,      &c->Qx,     &c->tempv,   &c->ATy,
                    &c->ATy_bar, &c->last_ATy, &c->ATdy, &c->QATdy,   &c->Rp,     &c->Rd,      &c->Ax,
                    &c->ftmp,   &c->ftmp2,  &c->vtmp_n, &c->vtmp_m,   &c->pz,     &c->pq,      &c->ptq,
-                   &c->d_red,  &c->d_red_out};
+                   &c->d_red,  &c->d_red_out, &c->d_red2};
   for (double** v : vs) {
     f(*v);
     *v = nullptr;
@@ -936,6 +936,7 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   HPR_TRY(dev_alloc_n(c, &c->g32_n, n));
   HPR_TRY(dev_alloc_n(c, &c->g32_m, m));
   HPR_TRY(zero_vec(c, &c->d_red_out, 64));
+  HPR_TRY(dev_alloc_n(c, &c->d_red2, (int64_t)kWideReduceCtas * kMaxRed));
   int64_t need = (int64_t)kRedGrid * kMaxRed;
   if (need > c->red_slots) {
     dev_free(c, c->d_red);
@@ -956,8 +957,10 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   c->precision = HPR_PREC_FP64;
   HPR_TRY(push_state(c));
   c->uploaded = true;
-  // the engine's tiled copies of the matrices (scaling rebuilds them in place)
-  HPR_TRY(prepare_engine(c));
+  // the arrays of the engine's tiled copies of the matrices, allocated here
+  // so that nothing allocates after the upload; the first engine use after
+  // the upload (normally after scaling) fills them
+  HPR_TRY(prepare_engine(c, false));
   HPR_CUDA(c, cudaStreamSynchronize(c->stream));
   c->scaled = false;
   c->upload_s = now_s() - t_up;

@@ -848,6 +848,30 @@ __global__ void __launch_bounds__(kThreads) final_reduce_kernel(const double* __
     for (int k = 0; k < NRED; ++k) out[k] = r.v[k];
 }
 
+// First level of a wide slot reduction: CTA b combines the contiguous chunk
+// [b * per, (b + 1) * per) of slots in a fixed order (per from nslots and
+// the grid size only) into partial slot b.
+constexpr int kWideReduceCtas = 148;
+template <int NRED, unsigned MASK>
+__global__ void __launch_bounds__(kThreads) slot_chunk_kernel(const double* __restrict__ slots, int nslots,
+                                                              double* __restrict__ partial) {
+  __shared__ double s_red[kMaxRed][kThreads / 32];
+  Red r;
+  red_init<NRED, MASK>(r);
+  const int per = (nslots + gridDim.x - 1) / gridDim.x;
+  const int b = blockIdx.x * per, e = b + per < nslots ? b + per : nslots;
+  for (int s = b + threadIdx.x; s < e; s += kThreads) {
+    Red o;
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) o.v[k] = slots[(int64_t)s * kMaxRed + k];
+    red_combine<NRED, MASK>(r, o);
+  }
+  block_reduce<NRED, MASK>(r, s_red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < NRED; ++k) partial[(int64_t)blockIdx.x * kMaxRed + k] = r.v[k];
+}
+
 template <int NRED, unsigned MASK, class F>
 __global__ void __launch_bounds__(kThreads) vec_reduce_kernel(int64_t n, F f, double* __restrict__ slots) {
   __shared__ double s_red[kMaxRed][kThreads / 32];

@@ -248,6 +248,7 @@ struct Ctx {
   double* d_red = nullptr;      // partial slots
   int64_t red_slots = 0;
   double* d_red_out = nullptr;  // final results (kMaxRed * 2)
+  double* d_red2 = nullptr;     // chunk sums of a two-level slot reduction (148 slots)
   double* h_red_out = nullptr;  // pinned
   DevState* d_state = nullptr;
   DevState* h_state = nullptr;  // pinned staging
@@ -295,9 +296,10 @@ int dev_alloc_n(Ctx* c, T** p, int64_t n) {
 int upload_plan(Ctx* c, Plan& p);
 // the plan's tiled copy of M (run layout), rebuilt when M's values changed;
 // refused inside a stream capture (it may allocate)
-int ensure_tiled(Ctx* c, const DevCSR& M, const Plan& p);
+// (build = false: only allocate the copy's arrays; its first use builds it)
+int ensure_tiled(Ctx* c, const DevCSR& M, const Plan& p, bool build = true);
 // ensure_tiled for every matrix side of the context
-int prepare_engine(Ctx* c);
+int prepare_engine(Ctx* c, bool build = true);
 PlanView view_of(const Plan& p, const int32_t* cone_start);
 int launch_iteration(Ctx* c, bool full);
 int run_iterations(Ctx* c, int64_t k, bool full_last);

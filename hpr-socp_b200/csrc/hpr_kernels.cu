@@ -147,7 +147,18 @@ int tile_layout(Ctx* c, const Plan& p, const int32_t* col, const T* val, int32_t
 }
 }  // namespace
 
-int ensure_tiled(Ctx* c, const DevCSR& M, const Plan& p) {
+int ensure_tiled(Ctx* c, const DevCSR& M, const Plan& p, bool build) {
+  if (!build) {
+    // allocate only (the first engine use builds the copy)
+    const int64_t ns = std::max<int64_t>(p.tslots, 1);
+    if (p.tiled_of != (const void*)&M) {
+      p.tiled_version = p.tiled_version32 = -1;
+      p.tiled_of = &M;
+    }
+    if (!p.d_tcol) HPR_TRY(dev_alloc_n(c, &p.d_tcol, ns));
+    if (!p.d_tval) HPR_TRY(dev_alloc_n(c, &p.d_tval, ns));
+    return HPR_OK;
+  }
   const bool want32 = M.val32 != nullptr || M.val16 != nullptr;
   const bool ok64 = p.tiled_of == (const void*)&M && p.tiled_version == M.version && p.d_tval;
   const bool ok32 = !want32 || (p.tiled_of == (const void*)&M && p.tiled_version32 == M.version32 &&
@@ -183,14 +194,14 @@ int ensure_tiled(Ctx* c, const DevCSR& M, const Plan& p) {
   return HPR_OK;
 }
 
-int prepare_engine(Ctx* c) {
+int prepare_engine(Ctx* c, bool build) {
   if (!c->uploaded) return HPR_OK;
-  HPR_TRY(ensure_tiled(c, c->AT, c->planX));
-  HPR_TRY(ensure_tiled(c, c->A, c->planY));
-  if (c->q_kind == HPR_Q_CSR || c->q_kind == HPR_Q_OPERATOR) HPR_TRY(ensure_tiled(c, c->Q, c->planQ));
+  HPR_TRY(ensure_tiled(c, c->AT, c->planX, build));
+  HPR_TRY(ensure_tiled(c, c->A, c->planY, build));
+  if (c->q_kind == HPR_Q_CSR || c->q_kind == HPR_Q_OPERATOR) HPR_TRY(ensure_tiled(c, c->Q, c->planQ, build));
   if (c->q_kind == HPR_Q_DIAG_LOWRANK) {
-    HPR_TRY(ensure_tiled(c, c->F, c->planF));
-    HPR_TRY(ensure_tiled(c, c->FT, c->planQ));
+    HPR_TRY(ensure_tiled(c, c->F, c->planF, build));
+    HPR_TRY(ensure_tiled(c, c->FT, c->planQ, build));
   }
   return HPR_OK;
 }
@@ -249,7 +260,7 @@ void launch_engine_prec(Ctx* c, int nt, const EngineArgs& a, const Epi& epi) {
 
 template <class Epi>
 int engine_launch(Ctx* c, const DevCSR& M, const Plan& p, const int32_t* cone_start, const double* xin,
-                  const float* xin32, const Epi& epi, bool bump, bool with_red, int red_off) {
+                  const float* xin32, const Epi& epi, bool bump, bool with_red, int red_off, bool wide_reduce = false) {
   int nt = (int)p.tasks.size();
   if (nt == 0) {
     if (bump) bump_inner_kernel<<<1, 32, 0, c->stream>>>(c->d_state);
@@ -277,9 +288,21 @@ int engine_launch(Ctx* c, const DevCSR& M, const Plan& p, const int32_t* cone_st
   c->launches++;
   HPR_CUDA(c, cudaGetLastError());
   if (with_red) {
-    final_reduce_kernel<Epi::kNRed, Epi::kMaxMask><<<1, kThreads, 0, c->stream>>>(c->d_red, p.nslots(),
-                                                                                   c->d_red_out + red_off);
-    c->launches++;
+    const int ns = p.nslots();
+    if (wide_reduce && ns > 2 * kThreads && c->d_red2) {
+      // two fixed-order levels: contiguous chunks of slots per CTA, then
+      // the chunk sums (one CTA reading tens of thousands of slots is a
+      // tenth of a power-iteration step on the benchmark)
+      const int g = std::min<int>(kWideReduceCtas, (ns + kThreads - 1) / kThreads);
+      slot_chunk_kernel<Epi::kNRed, Epi::kMaxMask><<<g, kThreads, 0, c->stream>>>(c->d_red, ns, c->d_red2);
+      final_reduce_kernel<Epi::kNRed, Epi::kMaxMask><<<1, kThreads, 0, c->stream>>>(c->d_red2, g,
+                                                                                     c->d_red_out + red_off);
+      c->launches += 2;
+    } else {
+      final_reduce_kernel<Epi::kNRed, Epi::kMaxMask><<<1, kThreads, 0, c->stream>>>(c->d_red, ns,
+                                                                                     c->d_red_out + red_off);
+      c->launches++;
+    }
     HPR_CUDA(c, cudaGetLastError());
   }
   return HPR_OK;
@@ -1131,7 +1154,8 @@ int power_two_pass_A(Ctx* c, int maxit, double tol, double* lam) {
       EpiPow ep{};
       ep.lin_src[0] = ep.cone_src[0] = zb[(cur + j) & 1];
       ep.out = zb[(cur + j + 1) & 1];
-      HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->ptq, nullptr, ep, false, true, kBase + 1 + 2 * j));
+      HPR_TRY(engine_launch(c, c->A, c->planY, c->d_con_start, c->ptq, nullptr, ep, false, true, kBase + 1 + 2 * j,
+                            true));
     }
     HPR_TRY(fetch_red(c, kBase + 1 + 2 * nb));
     double nz2 = c->h_red_out[kBase];
