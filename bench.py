@@ -33,6 +33,29 @@ WORKLOAD = ("sparse SOCP n=2,000,000 m=1,500,000 nnz(A)=25M (A1 1M lognormal row
             "var cones 100k x3 + 5k x50 + 20 x5000, con cones 100k x3 + 4k x50, Q=0")
 METRIC = "HPR iters/s"
 
+# --workload config2: the Q path at its configured size (one replica per GPU
+# too); the default line above is the benchmark workload
+WORKLOADS = {
+    "config1": {"workload": WORKLOAD, "seed": 1,
+                "l2": "inputs larger than L2 (A + A' ~ 600 MB)",
+                "kernel": "engine_kernel (x half-step over A' + y half-step over A, per iteration)",
+                "traffic_file": "engine_config1_dram_bytes.txt"},
+    "config2": {"workload": "QP-SOCP (robust portfolio) n=200,000 m=212,001 nnz(A)=4.4M, Q = D + F'F with F "
+                            "50 x n at 5% (never formed), box [0, 0.05], 2000 con cones x101",
+                "seed": 2,
+                "l2": "per-iteration streams ~186 MB (A + A' 106 MB) against the 126 MB L2: `value` is back to "
+                      "back iterations; `l2_flushed` times single iterations after a 512 MB write",
+                "kernel": "engine_kernel, 6 launches per iteration (F w; F'(.) + x/w step; F w_bar; "
+                          "F'(.) + tempv; A tempv + y step; A' y_bar + w2 step)",
+                "traffic_file": "engine_config2_dram_bytes.txt"},
+}
+
+
+def make_model(args):
+    from hprsocp_b200 import instances
+    gen = {"config1": instances.config1, "config2": instances.config2}[args.workload]
+    return gen(WORKLOADS[args.workload]["seed"], scale=args.scale)
+
 
 def measured_peak():
     """HBM copy bandwidth measured on this pool's B200s (MEASURED_PEAKS.json
@@ -148,6 +171,22 @@ def aggregate(world, steps, ms_max):
     return world * steps / (ms_max / 1e3)
 
 
+def l2_flushed_iterations(ctx, dev, count):
+    """Median device time (ms) of single partial iterations, each after a
+    512 MB write that evicts the L2, for workloads whose per-iteration
+    streams are within a small factor of the L2."""
+    import torch
+    buf = torch.empty(64 << 20, dtype=torch.float64, device=f"cuda:{dev}")
+    times = []
+    for i in range(count):
+        buf.fill_(float(i))
+        torch.cuda.synchronize(dev)
+        ctx.iterate(1, False)
+        times.append(ctx.last_iterate()[0])
+    del buf
+    return statistics.median(times)
+
+
 def cpu_iteration_rate(model, iters=3, threads=0):
     """Oracle (CPU restatement) iterations/s on this host's cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -166,7 +205,8 @@ def cpu_iteration_rate(model, iters=3, threads=0):
 
 def arm_config(args, world=1):
     """The `config` object both arms print (the driver compares them)."""
-    return {"workload": WORKLOAD, "precision": "fp64", "l2": "inputs larger than L2 (A + A' ~ 600 MB)",
+    w = WORKLOADS[args.workload]
+    return {"workload": w["workload"], "precision": "fp64", "l2": w["l2"],
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU", "scale": args.scale}
 
 
@@ -194,12 +234,12 @@ def run_reference(args, model, budget_s=150.0):
     loop_s = max(r.time - r.power_time, 1e-9)
     done = max(r.iter, 1)
     v = done / loop_s
-    sample = f"{r.iter} of {args.steps} HPR iterations of the benchmark instance, one full solve" + (
+    sample = f"{r.iter} of {args.steps} HPR iterations of the {args.workload} instance, one full solve" + (
         f" (stopped at the {budget_s:.0f} s bound)" if r.iter < args.steps else "")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "iter/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * loop_s / done,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded generator, seed 1)",
+            "data": f"synthetic (seeded generator, seed {WORKLOADS[args.workload]['seed']})",
             "config": arm_config(args, args.gpus),
             "path": "CPU restatement of the reference solver (oracle port), all host threads; no JIT, so the "
                     "warm-up steps do not apply",
@@ -279,6 +319,28 @@ def serving_measure(requests, slots=32, rate=0.0, baseline=60, resident=False, s
                               "how": "hpr_optimize per request, sequentially, after the server run "
                                      "and one untimed solve"},
             "speedup_vs_one_at_a_time": rate_s / seq_rate}
+
+
+def serving_in_fresh_process(requests, slots=32, baseline=30, timeout=900):
+    """`serving_measure` in a new process (``--mode serve``): the server
+    must create the process's CUDA context to get a hardware work queue per
+    slot and blocking waits, and this process already holds one."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--mode", "serve", "--requests", str(requests),
+           "--slots", str(slots), "--baseline", str(baseline)]
+    try:
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return {"error": f"serving run exceeded {timeout} s"}
+    lines = [ln for ln in out.stdout.strip().splitlines() if ln.startswith("{")]
+    if out.returncode != 0 or not lines:
+        return {"error": f"serving run failed (rc {out.returncode}): {out.stderr.strip()[-300:]}"}
+    d = json.loads(lines[-1])
+    keep = ("latency_s", "optimal", "mean_iterations", "mean_phase_s", "mean_loop_time_s", "one_at_a_time",
+            "speedup_vs_one_at_a_time")
+    res = {"solves_per_s": d["value"], "requests": d["steps"], "slots": d["config"]["slots"],
+           "device_resident_loop": d["config"]["device_resident_loop"], "arrival_rate": d["config"]["arrival_rate"]}
+    res.update({k: d[k] for k in keep})
+    return res
 
 
 def run_serving(args):
@@ -379,6 +441,8 @@ def main():
     ap.add_argument("--resident", action="store_true",
                     help="serve: small problems' solve loops in the device-resident request loop")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving summary of the default line")
+    ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS),
+                    help="iterate: config1 (the benchmark) or config2 (the Q path at n=200k)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.mode == "serve":
@@ -391,27 +455,29 @@ def main():
         run_spmv_baseline(args)
         return
 
-    from hprsocp_b200 import instances
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:
             return
-        model = instances.config1(1, scale=args.scale)
-        run_reference(args, model)
+        run_reference(args, make_model(args))
         return
 
     rank, world, dist = dist_init(args.gpus)
     import ctypes as C
     from hprsocp_b200 import Context, HPRSOCP_parameters, _abi
-    model = instances.config1(1, scale=args.scale)
+    model = make_model(args)
+    has_q = model.Q is not None or model.F is not None or model.q_diag is not None
+    if has_q:
+        args.no_serve = True  # the serving summary belongs to the benchmark line
     dev = int(os.environ.get("LOCAL_RANK", "0")) if dist is not None else 0
 
     # ---- device-resident iterations
     ctx = Context(model, device=dev)
     info = ctx.scale(HPRSOCP_parameters(verbose=False))
     lam = ctx.power_A() * 1.05
+    lamq = ctx.power_Q() * 1.05 if has_q else 0.0
     sigma = info["norm_b"] / info["norm_c"]
-    ctx.set_sigma_lambda(sigma, lam, 0.0)
+    ctx.set_sigma_lambda(sigma, lam, lamq)
     ctx.set_inner(0)
     with ClockSampler(dev) as clk:
         # clocks are sampled from the warm-up on; a timed region shorter than
@@ -426,6 +492,9 @@ def main():
         while clk.proc and clk.proc.poll() is None and len(clk.lines) - first < 2:
             ctx.iterate(20, False)
     clocks = clk.summary(first)
+    flushed = None
+    if has_q:
+        flushed = l2_flushed_iterations(ctx, dev, min(args.steps, 200))
     ms = dist_max(dist, ms)
     bytes_iter = ctx.iteration_bytes()
     ctx.close()
@@ -476,7 +545,7 @@ def main():
         # a fixed 200-request sample of the serving stream (config 4) through
         # the server, against one-at-a-time solves (before the CPU baseline,
         # whose host threads would compete with the server's)
-        serving = serving_measure(200, slots=32, baseline=30)
+        serving = serving_in_fresh_process(200, slots=32, baseline=30)
     cpu = None
     if not args.no_cpu:
         iters = 3
@@ -487,7 +556,7 @@ def main():
                               "cores": 1, "sample": "1 HPR iteration on one thread (the reference's CPU "
                                                     "path is single-threaded)"}}
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "engine_config1_dram_bytes.txt")
+    tfile = os.path.join(ROOT, "profiles", WORKLOADS[args.workload]["traffic_file"])
     if os.path.exists(tfile):
         try:
             traffic = float(open(tfile).read().split()[0])
@@ -496,19 +565,26 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per_iter_ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, seed 1)",
+        "vs_baseline": None, "dtype": "f64",
+        "data": f"synthetic (seeded generator, seed {WORKLOADS[args.workload]['seed']})",
         "config": arm_config(args, world),
         "hbm_gbs": achieved,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                      "algorithmic_bytes_per_iter": bytes_iter,
-                     "kernel": "engine_kernel (x half-step over A' + y half-step over A, per iteration)"},
+                     "kernel": WORKLOADS[args.workload]["kernel"]},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "serving": serving,
     }
+    if flushed is not None:
+        fl_ms = flushed / 1.0
+        line["l2_flushed"] = {"ms_per_step": fl_ms, "value": 1e3 / fl_ms, "unit": "iter/s",
+                              "hbm_gbs": bytes_iter / (fl_ms / 1e3) / 1e9,
+                              "what": "single iterations, each after a 512 MB device write that evicts L2, "
+                                      "timed with the iteration's CUDA events (launch latency included)"}
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

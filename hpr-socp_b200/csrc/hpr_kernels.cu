@@ -1324,10 +1324,11 @@ int repack_values(Ctx* c) {
   return HPR_OK;
 }
 
-// Algorithmic bytes of one partial no-Q iteration (roofline numerator):
+// Algorithmic bytes of one partial iteration (roofline numerator):
 //   sum over A, A' of nnz*(value + 4) + 4*(rows+1) + gathered vector once,
 //   plus the epilogue streams (x r/w, last_x, c, x_hat w; l, u on boxed
-//   variables; y r/w, last_y; AL, AU on linear rows; soc_rhs on cone rows).
+//   variables; y r/w, last_y; AL, AU on linear rows; soc_rhs on cone rows);
+//   on the Q path the two Q products and the wider epilogues as listed.
 double iteration_bytes(const Ctx* c) {
   double sv = c->precision == HPR_PREC_FP64 ? 8.0 : (c->precision == HPR_PREC_FP32 ? 4.0 : 2.0);
   double sg = c->precision == HPR_PREC_FP64 ? 8.0 : 4.0;
@@ -1335,9 +1336,30 @@ double iteration_bytes(const Ctx* c) {
   double m = (double)c->m, n = (double)c->n;
   double nb = (double)(((int64_t)c->h_var_idx.size() > 1) ? c->n_box : c->n);
   double b = 2.0 * nnz * (sv + 4.0) + 4.0 * (m + 1) + 4.0 * (n + 1) + sg * (m + n);
-  b += n * 40.0 + nb * 16.0;       // x r/w, last_x, c, x_hat w; l, u
-  b += m * 24.0 + (double)c->m_lin * 16.0 + (m - (double)c->m_lin) * 8.0;  // y r/w, last_y; AL, AU; rhs
-  if (c->precision != HPR_PREC_FP64) b += (n + m) * 4.0;  // FP32 copies written
+  if (!c->has_q) {
+    b += n * 40.0 + nb * 16.0;       // x r/w, last_x, c, x_hat w; l, u
+    b += m * 24.0 + (double)c->m_lin * 16.0 + (m - (double)c->m_lin) * 8.0;  // y r/w, last_y; AL, AU; rhs
+    if (c->precision != HPR_PREC_FP64) b += (n + m) * 4.0;  // FP32 copies written
+    return b;
+  }
+  // Q path (zxw1, tempv, y, w2 passes): two products with Q per iteration,
+  // Q w and Q w_bar.  Low rank: F v (k rows, gathers v, writes k values)
+  // then F'(.) (n rows, gathers the k values); a CSR Q (a caller's operator
+  // counts as its identity plan) streams Q and gathers v.
+  if (c->q_kind == HPR_Q_DIAG_LOWRANK) {
+    double nf = (double)c->F.nnz, k = (double)c->F.nrows;
+    b += 2.0 * (nf * 12.0 + 4.0 * (k + 1) + 8.0 * n + 8.0 * k);
+    b += 2.0 * (nf * 12.0 + 4.0 * (n + 1) + 8.0 * k);
+    b += 2.0 * 8.0 * n;  // qdiag read by the zxw1 and tempv passes
+  } else {
+    b += 2.0 * ((double)c->Q.nnz * 12.0 + 4.0 * (n + 1) + 8.0 * n);
+  }
+  b += n * 72.0 + nb * 16.0;  // zxw1: x, last_x, c, ATy, w r; l, u; w_bar, Qw, x, x_hat w
+  b += n * 32.0;              // tempv: x_hat, Qw, w_bar r; tempv w
+  b += n * 56.0;              // w2: w, w_bar, ATy, last_w, last_ATy r; w, ATy w
+  if (c->Q_is_diag) b += n * 24.0;  // fact1, fact2, fact
+  b += m * 32.0 + (double)c->m_lin * 16.0 + (m - (double)c->m_lin) * 8.0;  // y r/w, last_y, y_bar w; AL, AU; rhs
+  if (c->precision != HPR_PREC_FP64) b += (n + m) * 4.0;
   return b;
 }
 

@@ -94,3 +94,90 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+class ReplicatedServer:
+    """One `Server` per device, with each request routed to the device that
+    has the least outstanding work (the sum of nnz(A) + nnz(Q) + m + n over
+    its unfinished requests; ties go to the lowest device).  The serving
+    stream shards with no exchange between devices, so each device runs its
+    own server and the router only balances them.  Tickets are global:
+    ``poll`` finds the device that holds a ticket.
+
+    ``make_server(device)`` builds each device's server (default: ``Server``
+    with this object's slots, budget and mode); anything with ``submit``,
+    ``poll``, ``stats`` and ``close`` works, which is how the routing is
+    tested without a GPU."""
+
+    def __init__(self, devices, slots: int = 16, hbm_budget: int = 0, resident: bool = False, make_server=None):
+        self.devices = list(devices)
+        if not self.devices:
+            raise ValueError("ReplicatedServer needs at least one device")
+        if make_server is None:
+            def make_server(d):
+                return Server(slots=slots, device=d, hbm_budget=hbm_budget, resident=resident)
+        self.servers = []
+        try:
+            for d in self.devices:
+                self.servers.append(make_server(d))
+        except Exception:
+            self.close()
+            raise
+        self._load = [0] * len(self.servers)
+        self._where = {}  # global ticket -> (replica index, local ticket, work)
+        self._next = 0
+
+    @staticmethod
+    def work_of(model: SOCPModel) -> int:
+        w = int(model.A.nnz) + int(model.m) + int(model.n)
+        if model.Q is not None:
+            w += int(model.Q.nnz)
+        if model.F is not None:
+            w += 2 * int(model.F.nnz)
+        return w
+
+    def route(self) -> int:
+        """Replica index for the next request (least loaded first)."""
+        return min(range(len(self.servers)), key=lambda i: (self._load[i], i))
+
+    def submit(self, model: SOCPModel, params: Optional[HPRSOCP_parameters] = None) -> int:
+        work = self.work_of(model)
+        i = self.route()
+        local = self.servers[i].submit(model, params)
+        t = self._next
+        self._next += 1
+        self._where[t] = (i, local, work)
+        self._load[i] += work
+        return t
+
+    def device_of(self, ticket: int) -> int:
+        return self.devices[self._where[ticket][0]]
+
+    def poll(self, ticket: int, wait_ms: int = -1):
+        """(HPRSOCP_results, latency_s), or None if not finished within wait_ms."""
+        if ticket not in self._where:
+            raise _abi.HPRError(_abi.HPR_E_BAD_INPUT, f"unknown or already consumed ticket {ticket}")
+        i, local, work = self._where[ticket]
+        out = self.servers[i].poll(local, wait_ms)
+        if out is None:
+            return None
+        del self._where[ticket]
+        self._load[i] -= work
+        return out
+
+    def stats(self):
+        per = [s.stats() for s in self.servers]
+        tot = {k: sum(p[k] for p in per) for k in ("queued", "running", "reserved_bytes")}
+        tot["per_device"] = {d: p for d, p in zip(self.devices, per)}
+        return tot
+
+    def close(self):
+        for s in getattr(self, "servers", []):
+            s.close()
+        self.servers = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -415,8 +415,9 @@ void hpr_default_params(hpr_params* p);
  * total device milliseconds of the x- and y-half kernels.                  */
 int hpr_last_iterate_ms(hpr_ctx* ctx, double* ms_total, int64_t* launches);
 
-/* Algorithmic bytes moved by one partial iteration of the plain path (the
- * roofline numerator used by the benchmark).                               */
+/* Algorithmic bytes moved by one partial iteration (the roofline numerator
+ * used by the benchmark): the plain path, or the Q path's four passes with
+ * its two Q products when the problem has a Q.                             */
 int hpr_iteration_bytes(hpr_ctx* ctx, double* bytes_per_iter);
 
 

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from hprsocp_b200 import Context, HPRSOCP_parameters, _abi, instances
-from hprsocp_b200.serving import Server
+from hprsocp_b200.serving import ReplicatedServer, Server
 
 pytestmark = pytest.mark.gpu
 
@@ -102,3 +102,17 @@ def test_a_ticket_is_consumed_by_its_poll(stream):
         import ctypes as C
         lat = C.c_double()
         assert srv.lib.hpr_serve_poll(srv.h, t, 0, None, C.byref(lat)) == _abi.HPR_E_BAD_INPUT
+
+
+def test_replicated_servers_give_the_single_server_results(stream):
+    """Requests routed across replicas (two servers on device 0 here, one
+    per GPU in production) give the bits a single server gives."""
+    with Server(slots=8) as srv:
+        single = [srv.poll(t)[0] for t in [srv.submit(m, _params(tol)) for m, tol, _ in stream[:12]]]
+    with ReplicatedServer([0, 0], slots=4) as rs:
+        tickets = [rs.submit(m, _params(tol)) for m, tol, _ in stream[:12]]
+        assert {rs.device_of(t) for t in tickets} == {0} and min(rs._load) > 0
+        routed = [rs.poll(t)[0] for t in tickets]
+    for a, b in zip(single, routed):
+        assert a.status == b.status == "OPTIMAL" and a.iter == b.iter
+        assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y)
