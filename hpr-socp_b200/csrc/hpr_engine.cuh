@@ -491,11 +491,15 @@ __device__ __forceinline__ void long_row_part(const EngineArgs& a, Epi& epi, int
   }
   if (__shfl_sync(0xffffffffu, last, 0)) {
     __threadfence();
+    // the lanes load 32 partials at a time and the sum takes them in slice
+    // order from the lanes (one L2 round trip per 32 slices)
     double tot = 0.0;
-    if (lane == 0) {
-      for (int p = 0; p < lr.nparts; ++p) tot = tot + __ldcg(a.pv.partials + lr.partial_base + p);
-      a.pv.lng_cnt[t.group] = 0;
+    for (int p0 = 0; p0 < lr.nparts; p0 += 32) {
+      const int cnt = min(32, lr.nparts - p0);
+      const double mine = lane < cnt ? __ldcg(a.pv.partials + lr.partial_base + p0 + lane) : 0.0;
+      for (int j = 0; j < cnt; ++j) tot = tot + __shfl_sync(0xffffffffu, mine, j);
     }
+    if (lane == 0) a.pv.lng_cnt[t.group] = 0;
     const bool to_cone = Epi::kCones && lr.bigcone >= 0;
     Red lred;
     red_init<Epi::kNRed, Epi::kMaxMask>(lred);
