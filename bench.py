@@ -551,7 +551,7 @@ def main():
         iters = 3
         cpu_rate = cpu_iteration_rate(model, iters=iters, threads=0)
         cpu = {"value": cpu_rate, "unit": "iter/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"{iters} HPR iterations of the benchmark instance on the oracle (all host threads)",
+               "sample": f"{iters} HPR iterations of the {args.workload} instance on the oracle (all host threads)",
                "one_thread": {"value": cpu_iteration_rate(model, iters=1, threads=1), "unit": "iter/s",
                               "cores": 1, "sample": "1 HPR iteration on one thread (the reference's CPU "
                                                     "path is single-threaded)"}}

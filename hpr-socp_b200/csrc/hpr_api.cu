@@ -873,15 +873,7 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
     HPR_TRY(put_vec(c, &c->qdiag, p->q_diag, n));
     c->has_q = true;
     qrp = ftrp;
-    // F has few rows (tens) of many nonzeros each: at full tiles its
-    // products occupy a fraction of the warps and each warp's chain of
-    // steps sets the launch's time, so F's tiles are cut to give every
-    // resident warp (3 CTAs of 8 warps per SM) about one
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    const int64_t warps = (int64_t)sms * 3 * 8;
-    const int fcap = (int)std::max<int64_t>(64, std::min<int64_t>(kNnzTile, c->F.nnz / warps));
-    build_plan(frp, k, {}, c->planF, fcap);
+    build_plan(frp, k, {}, c->planF);
     HPR_TRY(upload_plan(c, c->planF));
   } else if (p->q_kind != HPR_Q_NONE) {
     return set_err(c, HPR_E_BAD_INPUT, "unknown q_kind");

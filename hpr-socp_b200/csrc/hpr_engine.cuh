@@ -4,31 +4,34 @@
 // each result to an epilogue functor, so intermediate vectors (A'y, A x_hat,
 // z_raw, s_raw) never reach HBM.  Work comes from the host planner
 // (hpr_plan.cpp) as cone-aligned warp tiles of at most kNnzTile nonzeros and
-// kRowCap rows.
+// kRowCap rows, stored in the run layout (TileRun, hpr_internal.h): a tile's
+// nonzeros cut into 32 contiguous runs, lane-interleaved.
 //
 // Every warp works on its own tiles with no CTA-wide synchronisation, so the
 // SM's 24 resident warps hide each other's memory latency.  Persistent
-// warps take tiles (kGrab at a time) from an atomic counter; per tile a warp
-//   0. loads its rows' row pointers (two rows per lane) into registers;
-//   1. streams the tile's column indices and values with coalesced
-//      evict-first loads, gathers xin through L2 (ld.global.cg) and writes the
-//      products to a warp-private shared-memory buffer, then requests the
-//      rows' epilogue inputs (HPR_ENGINE_PREFETCH=1 requests them in step 0,
-//      which costs registers during the gathers);
-//   2. sums each row from shared memory in ascending column order by one
-//      lane (rows of at most kSerialMax nonzeros — bit-identical to the
-//      reference's sequential sparse product) or by the whole warp;
-//   3. runs the epilogue per row (linear rows / boxed variables) or per cone
-//      (one lane per cone computes ||tail||_2 serially, then one lane per row
-//      projects).  Cones larger than one warp tile and rows longer than one
-//      tile are split over several tiles; the warp that completes the last
-//      slice (atomic arrival counter, no waiting) finishes them;
+// warps take their first tile by warp index (plans without split cones) and
+// the rest from an atomic counter; per tile a warp
+//   1. streams its run's column indices and values with coalesced
+//      evict-first loads, gathers xin through L2 (ld.global.cg) and adds the
+//      products of each row inside the run in column order in a register,
+//      closing a row's sum into a shared-memory slot at the next row start;
+//   2. adds the parts of rows that span runs with a fixed-order segmented
+//      scan over the lanes, and hands each row's sum to the lane that owns
+//      the row (two rows per lane);
+//   3. requests the rows' epilogue inputs and runs the epilogue per row
+//      (linear rows / boxed variables) or per cone (one lane per cone
+//      computes ||tail||_2 serially, then one lane per row projects).  Rows
+//      longer than one tile are split over several tiles, and the warp that
+//      completes the last slice (atomic arrival counter, no waiting) finishes
+//      them.  Cones larger than one tile are split into slices that store
+//      their shares of the norm; the last slice publishes the norm and apply
+//      tiles, queued after every other tile, project the rows (a bounded wait
+//      for the published norm);
 //   4. reduces optional scalar reductions in a fixed order and writes one
 //      slot per tile, so results do not depend on scheduling.
-// The last warp to finish resets the tile counter and may advance the
+// The last CTA to finish resets the tile counter and may advance the
 // Halpern counter `inner`, so a whole iteration runs from device-resident
-// scalars and can be captured in a CUDA graph.  No warp ever waits on
-// another, so the kernel cannot deadlock.
+// scalars and can be captured in a CUDA graph.
 #pragma once
 
 #include "hpr_internal.h"
@@ -760,7 +763,17 @@ struct EngineChunk {
   static constexpr int value = kChunk;
 };
 
-template <class Epi, int PREC>
+// kStatic (host-chosen, only for plans without split cones): first tiles by
+// warp index, the rest from the atomic counter counted from nstat, so a
+// short launch pays no burst of same-address atomics before its first tile
+// (when the static tiles are all the tiles no warp touches the counter),
+// and one arrival per CTA on the done counter.  Plans with split cones take
+// every tile from the counter: a cone's apply tile waits for its slices,
+// and a slice taken from the counter is always on a running warp, while a
+// static slice may belong to a CTA that is not resident yet.  (Measured on
+// B200: the static form is 3-4% faster on the Q path's short launches and
+// 0.5% slower on the benchmark's long ones, so each plan gets its form.)
+template <class Epi, int PREC, bool kStatic>
 __global__ void __launch_bounds__(kEngineThreads, EngineMinBlocks<Epi>::value) engine_kernel(EngineArgs a, Epi epi) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmem* s_ws = reinterpret_cast<WarpSmem*>(smem_raw);
@@ -773,38 +786,71 @@ __global__ void __launch_bounds__(kEngineThreads, EngineMinBlocks<Epi>::value) e
   const int ntasks = a.pv.ntasks;
   epi.setup(a.st);
   WarpSmem& ws = s_ws[wid];
-  int base = 0;
-  if (lane == 0) base = atomicAdd(a.pv.task_ctr, kGrab);
-  base = __shfl_sync(0xffffffffu, base, 0);
-  while (base < ntasks) {
-    // with HPR_ENGINE_EARLYGRAB the next grab is requested before this one is
-    // processed, so its atomic latency is hidden behind the tiles
-    int next = 0;
-    if (HPR_ENGINE_EARLYGRAB && lane == 0) next = atomicAdd(a.pv.task_ctr, kGrab);
-    for (int q = 0; q < kGrab && base + q < ntasks; ++q) {
-      int pf = -1;
-      if (HPR_ENGINE_L2PF >= 2 && HPR_ENGINE_EARLYGRAB && q == kGrab - 1) {
-        pf = __shfl_sync(0xffffffffu, next, 0);
-        pf = pf < ntasks ? pf : -1;
-      }
-      process_warp_tile<Epi, PREC, false, EngineChunk<Epi>::value>(a, epi, base + q, ws, pf);
+  if constexpr (kStatic) {
+    const int nstat = a.pv.nbig == 0 ? min(ntasks, (int)gridDim.x * kWarpsPerCta * kGrab) : 0;
+    const bool dyn = nstat < ntasks;
+    int base = (blockIdx.x * kWarpsPerCta + wid) * kGrab;
+    if (base >= nstat) {
+      base = ntasks;
+      if (dyn && lane == 0) base = nstat + atomicAdd(a.pv.task_ctr, kGrab);
+      base = __shfl_sync(0xffffffffu, base, 0);
     }
-    if (!HPR_ENGINE_EARLYGRAB && lane == 0) next = atomicAdd(a.pv.task_ctr, kGrab);
-    base = __shfl_sync(0xffffffffu, next, 0);
+    while (base < ntasks) {
+      for (int q = 0; q < kGrab && base + q < ntasks; ++q)
+        process_warp_tile<Epi, PREC, false, EngineChunk<Epi>::value>(a, epi, base + q, ws);
+      int next = ntasks;
+      if (dyn && lane == 0) next = nstat + atomicAdd(a.pv.task_ctr, kGrab);
+      base = __shfl_sync(0xffffffffu, next, 0);
+    }
+  } else {
+    int base = 0;
+    if (lane == 0) base = atomicAdd(a.pv.task_ctr, kGrab);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    while (base < ntasks) {
+      // with HPR_ENGINE_EARLYGRAB the next grab is requested before this one
+      // is processed, so its atomic latency is hidden behind the tiles
+      int next = 0;
+      if (HPR_ENGINE_EARLYGRAB && lane == 0) next = atomicAdd(a.pv.task_ctr, kGrab);
+      for (int q = 0; q < kGrab && base + q < ntasks; ++q) {
+        int pf = -1;
+        if (HPR_ENGINE_L2PF >= 2 && HPR_ENGINE_EARLYGRAB && q == kGrab - 1) {
+          pf = __shfl_sync(0xffffffffu, next, 0);
+          pf = pf < ntasks ? pf : -1;
+        }
+        process_warp_tile<Epi, PREC, false, EngineChunk<Epi>::value>(a, epi, base + q, ws, pf);
+      }
+      if (!HPR_ENGINE_EARLYGRAB && lane == 0) next = atomicAdd(a.pv.task_ctr, kGrab);
+      base = __shfl_sync(0xffffffffu, next, 0);
+    }
   }
 #if HPR_ENGINE_PDL
   // no more tiles for this warp: the next kernel may start being scheduled
   asm volatile("griddepcontrol.launch_dependents;");
 #endif
-  // ---- last warp: reset the tile counter, advance the Halpern counter
-  if (lane == 0) {
-    __threadfence();
-    int tk = atomicAdd(a.pv.done_ctr, 1);
-    if (tk == (int)(gridDim.x * kWarpsPerCta) - 1) {
-      *a.pv.task_ctr = 0;
-      *a.pv.done_ctr = 0;
-      if (a.bump_inner) a.st->inner = a.st->inner + 1;
+  // ---- last arrival: reset the tile counter, advance the Halpern counter
+  if constexpr (kStatic) {
+    // one arrival per CTA, once all of its warps are past their last grab
+    __syncthreads();
+    if (threadIdx.x == 0) {
       __threadfence();
+      int tk = atomicAdd(a.pv.done_ctr, 1);
+      if (tk == (int)gridDim.x - 1) {
+        *a.pv.task_ctr = 0;
+        *a.pv.done_ctr = 0;
+        if (a.bump_inner) a.st->inner = a.st->inner + 1;
+        __threadfence();
+      }
+    }
+  } else {
+    if (lane == 0) {
+      __threadfence();
+      int tk = atomicAdd(a.pv.done_ctr, 1);
+      if (tk == (int)(gridDim.x * kWarpsPerCta) - 1) {
+        *a.pv.task_ctr = 0;
+        *a.pv.done_ctr = 0;
+        if (a.bump_inner) a.st->inner = a.st->inner + 1;
+        __threadfence();
+      }
     }
   }
 }

@@ -210,14 +210,14 @@ namespace {
 
 // Persistent grid size of one engine instantiation (resident CTAs per SM x
 // SMs), computed once.
-template <class Epi, int PREC>
+template <class Epi, int PREC, bool kStatic>
 int engine_grid(int* smem_bytes) {
   static std::once_flag once;
   static int grid = 1;
   constexpr int dyn = kEngineSmem;
   *smem_bytes = dyn;
   std::call_once(once, [] {
-    auto k = engine_kernel<Epi, PREC>;
+    auto k = engine_kernel<Epi, PREC, kStatic>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     const int carve = HPR_ENGINE_CARVEOUT >= 0 ? (int)(HPR_ENGINE_CARVEOUT)
                                                : engine_carveout(EngineMinBlocks<Epi>::value);
@@ -233,10 +233,10 @@ int engine_grid(int* smem_bytes) {
 
 // One warp per tile at most: a small problem occupies only the SMs it needs,
 // so other streams (other contexts of a serving process) run beside it.
-template <class Epi, int PREC>
-void launch_engine_prec(Ctx* c, int nt, const EngineArgs& a, const Epi& epi) {
+template <class Epi, int PREC, bool kStatic>
+void launch_engine_form(Ctx* c, int nt, const EngineArgs& a, const Epi& epi) {
   int dyn = 0;
-  const int full = engine_grid<Epi, PREC>(&dyn);
+  const int full = engine_grid<Epi, PREC, kStatic>(&dyn);
   const int g = std::max(1, std::min(full, (nt + kWarpsPerCta - 1) / kWarpsPerCta));
 #if HPR_ENGINE_PDL
   // programmatic dependent launch: the kernel may be scheduled while the
@@ -252,10 +252,19 @@ void launch_engine_prec(Ctx* c, int nt, const EngineArgs& a, const Epi& epi) {
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, engine_kernel<Epi, PREC>, a, epi);
+  cudaLaunchKernelEx(&cfg, engine_kernel<Epi, PREC, kStatic>, a, epi);
 #else
-  engine_kernel<Epi, PREC><<<g, kEngineThreads, dyn, c->stream>>>(a, epi);
+  engine_kernel<Epi, PREC, kStatic><<<g, kEngineThreads, dyn, c->stream>>>(a, epi);
 #endif
+}
+
+// Plans without split cones take their first tiles by warp index
+// (engine_kernel's kStatic form); the others take every tile from the
+// counter.
+template <class Epi, int PREC>
+void launch_engine_prec(Ctx* c, int nt, const EngineArgs& a, const Epi& epi) {
+  if (a.pv.nbig == 0) launch_engine_form<Epi, PREC, true>(c, nt, a, epi);
+  else launch_engine_form<Epi, PREC, false>(c, nt, a, epi);
 }
 
 template <class Epi>
