@@ -123,21 +123,15 @@ void free_all(Ctx* c) {
   c->uploaded = c->scaled = false;
 }
 
-bool finite_all(const double* v, int64_t n) {
-  for (int64_t i = 0; i < n; ++i)
-    if (!std::isfinite(v[i])) return false;
-  return true;
-}
-bool nonan_all(const double* v, int64_t n) {
-  for (int64_t i = 0; i < n; ++i)
-    if (std::isnan(v[i])) return false;
-  return true;
-}
+bool is_finite(double x) { return std::isfinite(x); }
+bool not_nan(double x) { return !std::isnan(x); }
+bool finite_all(const double* v, int64_t n) { return host_all(v, n, is_finite); }
+bool nonan_all(const double* v, int64_t n) { return host_all(v, n, not_nan); }
 
 int put_vec(Ctx* c, double** d, const double* h, int64_t n) {
   HPR_TRY(dev_alloc_n(c, d, n));
   if (n > 0) {
-    if (h) HPR_CUDA(c, cudaMemcpyAsync(*d, h, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (h) HPR_TRY(h2d_copy(c, *d, h, (size_t)n * sizeof(double)));
     else HPR_CUDA(c, cudaMemsetAsync(*d, 0, n * sizeof(double), c->stream));
   }
   return HPR_OK;
@@ -850,8 +844,6 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   } else {
     HPR_TRY(transpose_csr(c, c->A, c->AT, trp));
   }
-  c->h_A_rowptr = rp;
-  c->h_AT_rowptr = trp;
   // Q
   c->q_kind = p->q_kind;
   c->has_q = false;
@@ -896,14 +888,18 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   // HPR_SMALL_TILE nonzeros: they occupy few warps, so shorter tiles shorten
   // each launch's longest chain (0: every problem uses full tiles)
   const int cap = c->A.nnz < (int64_t)HPR_SMALL_PLAN_NNZ ? (int)HPR_SMALL_TILE : 0;
-  build_plan(trp, n, vcones, c->planX, cap);
-  build_plan(rp, m, ccones, c->planY, cap);
+  // the plans of A', A (and Q) are independent host work: built side by side
+  {
+    std::thread ty([&] { build_plan(rp, m, ccones, c->planY, cap); });
+    std::thread tq;
+    if (c->has_q) tq = std::thread([&] { build_plan(qrp, n, vcones, c->planQ, cap); });
+    build_plan(trp, n, vcones, c->planX, cap);
+    ty.join();
+    if (tq.joinable()) tq.join();
+  }
   HPR_TRY(upload_plan(c, c->planX));
   HPR_TRY(upload_plan(c, c->planY));
-  if (c->has_q) {
-    build_plan(qrp, n, vcones, c->planQ, cap);
-    HPR_TRY(upload_plan(c, c->planQ));
-  }
+  if (c->has_q) HPR_TRY(upload_plan(c, c->planQ));
   // problem vectors
   HPR_TRY(put_vec(c, &c->c, p->c, n));
   HPR_TRY(put_vec(c, &c->l, p->l, n));

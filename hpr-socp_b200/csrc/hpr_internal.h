@@ -107,7 +107,7 @@ struct Plan {
   int32_t* d_lng_cnt = nullptr;
   double* d_partials = nullptr;  // long-row partial sums
   double* d_raw = nullptr;       // big-cone raw values (nrows)
-  int32_t* d_ctr = nullptr;      // [0] tile counter, [1] finished warps
+  int32_t* d_ctr = nullptr;      // [0] tile counter, [1] finished warps (CTAs in the static form)
   TileRun* d_runs = nullptr;
   uint32_t* d_desc = nullptr;
   double* d_cpart = nullptr;      // big-cone norm shares per slice
@@ -171,7 +171,7 @@ struct PlanView {
   double* raw;
   const int32_t* cone_start;  // cone start rows (+ sentinel), this side
   int32_t* task_ctr;          // next tile to take
-  int32_t* done_ctr;          // CTAs that finished (last one resets both)
+  int32_t* done_ctr;          // warps (CTAs in the static form) that finished; the last resets both
   double* cpart;
   double* bignorm;
   int32_t* big_ready;
@@ -200,7 +200,6 @@ struct Ctx {
   int q_kind = HPR_Q_NONE;
   bool has_q = false, Q_is_diag = false;
   DevCSR A, AT, Q, F, FT;
-  std::vector<int32_t> h_A_rowptr, h_AT_rowptr;
   std::vector<int64_t> h_con_idx, h_var_idx;  // 0-based starts + sentinel
   int32_t* d_con_start = nullptr;  // int32 copies (+ sentinel)
   int32_t* d_var_start = nullptr;
@@ -327,6 +326,15 @@ int upload_csr(Ctx* c, const hpr_csr& s, int base, int64_t nr, int64_t nc, const
                std::vector<int32_t>& rp);
 // deterministic transpose on the device; trp receives T's row pointers
 int transpose_csr(Ctx* c, const DevCSR& M, DevCSR& T, std::vector<int32_t>& trp);
+// host-to-device copy of a pageable host array, enqueued on the context's
+// stream: large arrays go through pinned chunks filled by several host
+// threads (the source may be reused as soon as this returns)
+int h2d_copy(Ctx* c, void* dst, const void* src, size_t bytes);
+// device-to-host copy into a pageable host array after the work enqueued on
+// the context's stream; returns once the data is in dst
+int d2h_copy(Ctx* c, void* dst, const void* src, size_t bytes);
+// pred(v[i]) for every i, checked on several host threads for long arrays
+bool host_all(const double* v, int64_t n, bool (*pred)(double));
 // scaling (hpr_scale.cu)
 int run_scaling(Ctx* c, const hpr_params* p, hpr_scale_info* out);
 

@@ -1214,25 +1214,21 @@ int launch_unscale(Ctx* c, double* hx, double* hy, double* hz, double* hw) {
   size_t nb = (size_t)c->n * sizeof(double);
   if (hx || (hw && !c->has_q)) {
     HPR_TRY(vec_map(c, c->n, [=] __device__(int64_t i) { t[i] = bs * (xb[i] / col[i]); }));
-    if (hx) HPR_CUDA(c, cudaMemcpyAsync(hx, t, nb, cudaMemcpyDeviceToHost, c->stream));
-    if (hw && !c->has_q) HPR_CUDA(c, cudaMemcpyAsync(hw, t, nb, cudaMemcpyDeviceToHost, c->stream));
-    HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (hx) HPR_TRY(d2h_copy(c, hx, t, nb));
+    if (hw && !c->has_q) HPR_TRY(d2h_copy(c, hw, t, nb));
   }
   if (hw && c->has_q) {
     HPR_TRY(vec_map(c, c->n, [=] __device__(int64_t i) { t[i] = bs * (wb[i] / col[i]); }));
-    HPR_CUDA(c, cudaMemcpyAsync(hw, t, nb, cudaMemcpyDeviceToHost, c->stream));
-    HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+    HPR_TRY(d2h_copy(c, hw, t, nb));
   }
   if (hz) {
     HPR_TRY(vec_map(c, c->n, [=] __device__(int64_t i) { t[i] = cs * (zb[i] * col[i]); }));
-    HPR_CUDA(c, cudaMemcpyAsync(hz, t, nb, cudaMemcpyDeviceToHost, c->stream));
-    HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+    HPR_TRY(d2h_copy(c, hz, t, nb));
   }
   if (hy && c->m > 0) {
     double* tm = c->vtmp_m;
     HPR_TRY(vec_map(c, c->m, [=] __device__(int64_t i) { tm[i] = cs * (yb[i] / row[i]); }));
-    HPR_CUDA(c, cudaMemcpyAsync(hy, tm, (size_t)c->m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    HPR_CUDA(c, cudaStreamSynchronize(c->stream));
+    HPR_TRY(d2h_copy(c, hy, tm, (size_t)c->m * sizeof(double)));
   }
   return HPR_OK;
 }

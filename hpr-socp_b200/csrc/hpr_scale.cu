@@ -117,42 +117,93 @@ bool uses_pre_pock(int st) {
          st == HPR_SOC_SCALE_COUNT_AWARE_SMALL_CONE_BIAS;
 }
 
+// The three kernels below give each row (or cone) a group of G lanes that
+// walk its entries with stride G, so a warp's loads are coalesced and a long
+// row or cone is spread over G lanes instead of one thread.  G is chosen per
+// launch from the mean length (group_lanes).  Maxima do not depend on the
+// order; sums are added per lane and then over the group in a fixed shuffle
+// order, so the result depends on the data and G only.
+template <int G>
+__device__ __forceinline__ double group_combine(double v, bool sum) {
+#pragma unroll
+  for (int off = G / 2; off > 0; off >>= 1) {
+    const double o = __shfl_down_sync(0xffffffffu, v, off, G);
+    if (((threadIdx.x & 31) % G) + off < G) v = sum ? v + o : cmax(v, o);
+  }
+  return v;
+}
+
 // compute_row_max_abs(_with_Q)_kernel! / compute_row_sum_abs_kernel! /
 // compute_col_sum_abs_with_Q_kernel! (kernels.jl:6699-6798, 6965-7030)
+template <int G>
 __global__ void row_stat_kernel(int64_t nr, const int32_t* rp, const double* v, const int32_t* qrp,
                                 const double* qv, int use_sum, double* out) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += (int64_t)gridDim.x * blockDim.x) {
+  constexpr int kRows = 32 / G;  // rows per warp step
+  const int lane = threadIdx.x & 31, sub = lane % G;
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t b0 = w * kRows; b0 < nr; b0 += nw * kRows) {
+    const int64_t i = b0 + lane / G;
     double q = 0.0, a = 0.0;
-    if (qrp)
-      for (int64_t k = qrp[i]; k < qrp[i + 1]; ++k) q = use_sum ? q + fabs(qv[k]) : cmax(q, fabs(qv[k]));
-    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) a = use_sum ? a + fabs(v[k]) : cmax(a, fabs(v[k]));
-    double r = use_sum ? q + a : cmax(q, a);
-    out[i] = clamp4(r > 0.0 ? sqrt(r) : 1.0);
+    if (i < nr) {
+      if (qrp)
+        for (int64_t k = qrp[i] + sub; k < qrp[i + 1]; k += G) q = use_sum ? q + fabs(qv[k]) : cmax(q, fabs(qv[k]));
+      for (int64_t k = rp[i] + sub; k < rp[i + 1]; k += G) a = use_sum ? a + fabs(v[k]) : cmax(a, fabs(v[k]));
+    }
+    q = group_combine<G>(q, use_sum != 0);
+    a = group_combine<G>(a, use_sum != 0);
+    if (i < nr && sub == 0) {
+      const double r = use_sum ? q + a : cmax(q, a);
+      out[i] = clamp4(r > 0.0 ? sqrt(r) : 1.0);
+    }
   }
 }
 
 // apply_soc_block_scaling(_phase_taper)_kernel! (kernels.jl:6820-6920)
+template <int G>
 __global__ void block_kernel(int64_t ncones, const int32_t* cs, double* t, int st, int ph, int loc) {
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < ncones; k += (int64_t)gridDim.x * blockDim.x) {
-    int64_t a = cs[k], b = cs[k + 1], len = b - a;
-    if (len <= 0) continue;
+  constexpr int kCones = 32 / G;
+  const int lane = threadIdx.x & 31, sub = lane % G;
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t b0 = w * kCones; b0 < ncones; b0 += nw * kCones) {
+    const int64_t k = b0 + lane / G;
+    int64_t a = 0, b = 0;
+    if (k < ncones) {
+      a = cs[k];
+      b = cs[k + 1];
+    }
     double bmax = 0.0, ss = 0.0;
-    for (int64_t j = a; j < b; ++j) {
+    for (int64_t j = a + sub; j < b; j += G) {
       bmax = cmax(bmax, t[j]);
       ss = fma(t[j], t[j], ss);
     }
-    double rms = st == HPR_SOC_SCALE_MAX ? bmax : sqrt(ss / (double)len);
-    double v = block_value(len, bmax, rms, st, ph, loc, ncones);
-    for (int64_t j = a; j < b; ++j) t[j] = v;
+    // every lane of the group has read its entries before any is written
+    bmax = group_combine<G>(bmax, false);
+    ss = group_combine<G>(ss, true);
+    bmax = __shfl_sync(0xffffffffu, bmax, lane - sub);
+    ss = __shfl_sync(0xffffffffu, ss, lane - sub);
+    const int64_t len = b - a;
+    if (len <= 0) continue;
+    const double rms = st == HPR_SOC_SCALE_MAX ? bmax : sqrt(ss / (double)len);
+    const double val = block_value(len, bmax, rms, st, ph, loc, ncones);
+    for (int64_t j = a + sub; j < b; j += G) t[j] = val;
   }
 }
 
 // scale_csr_row_col_kernel! (kernels.jl:7120-7140)
+template <int G>
 __global__ void scale_csr_kernel(int64_t nr, const int32_t* rp, const int32_t* ci, double* v, const double* r,
                                  const double* cl) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += (int64_t)gridDim.x * blockDim.x) {
-    double rinv = 1.0 / r[i];
-    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+  constexpr int kRows = 32 / G;
+  const int lane = threadIdx.x & 31, sub = lane % G;
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t b0 = w * kRows; b0 < nr; b0 += nw * kRows) {
+    const int64_t i = b0 + lane / G;
+    if (i >= nr) continue;
+    const double rinv = 1.0 / r[i];
+    for (int64_t k = rp[i] + sub; k < rp[i + 1]; k += G) {
       double x = v[k];
       x *= rinv;
       x /= cl[ci[k]];
@@ -234,6 +285,46 @@ int bnorms(Ctx* c, double* inf_, double* l2_) {
 
 inline int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
 
+// lanes per row (or cone) for a mean length of `mean` entries
+inline int group_lanes(double mean) { return mean <= 6.0 ? 4 : (mean <= 12.0 ? 8 : (mean <= 24.0 ? 16 : 32)); }
+
+template <int G>
+void row_stat_g(Ctx* c, int64_t nr, const int32_t* rp, const double* v, const int32_t* qrp, const double* qv,
+                int use_sum, double* out) {
+  row_stat_kernel<G><<<grid_for(nr * G), 256, 0, c->stream>>>(nr, rp, v, qrp, qv, use_sum, out);
+}
+void row_stat(Ctx* c, int64_t nr, int64_t nnz, const int32_t* rp, const double* v, const int32_t* qrp,
+              const double* qv, int use_sum, double* out) {
+  switch (group_lanes((double)nnz / (double)std::max<int64_t>(nr, 1))) {
+    case 4: row_stat_g<4>(c, nr, rp, v, qrp, qv, use_sum, out); break;
+    case 8: row_stat_g<8>(c, nr, rp, v, qrp, qv, use_sum, out); break;
+    case 16: row_stat_g<16>(c, nr, rp, v, qrp, qv, use_sum, out); break;
+    default: row_stat_g<32>(c, nr, rp, v, qrp, qv, use_sum, out); break;
+  }
+}
+void block_scale(Ctx* c, int64_t ncones, int64_t len, const int32_t* cs, double* t, int st, int ph, int loc) {
+  const int g = group_lanes((double)len / (double)std::max<int64_t>(ncones, 1));
+  const int grid = grid_for(ncones * g);
+  switch (g) {
+    case 4: block_kernel<4><<<grid, 256, 0, c->stream>>>(ncones, cs, t, st, ph, loc); break;
+    case 8: block_kernel<8><<<grid, 256, 0, c->stream>>>(ncones, cs, t, st, ph, loc); break;
+    case 16: block_kernel<16><<<grid, 256, 0, c->stream>>>(ncones, cs, t, st, ph, loc); break;
+    default: block_kernel<32><<<grid, 256, 0, c->stream>>>(ncones, cs, t, st, ph, loc); break;
+  }
+}
+void scale_csr(Ctx* c, const DevCSR& M, const double* r, const double* cl) {
+  const int64_t nr = M.nrows;
+  if (nr == 0) return;
+  const int g = group_lanes((double)M.nnz / (double)nr);
+  const int grid = grid_for(nr * g);
+  switch (g) {
+    case 4: scale_csr_kernel<4><<<grid, 256, 0, c->stream>>>(nr, M.rowptr, M.col, M.val, r, cl); break;
+    case 8: scale_csr_kernel<8><<<grid, 256, 0, c->stream>>>(nr, M.rowptr, M.col, M.val, r, cl); break;
+    case 16: scale_csr_kernel<16><<<grid, 256, 0, c->stream>>>(nr, M.rowptr, M.col, M.val, r, cl); break;
+    default: scale_csr_kernel<32><<<grid, 256, 0, c->stream>>>(nr, M.rowptr, M.col, M.val, r, cl); break;
+  }
+}
+
 int scale_pass(Ctx* c, int st, int phase, int use_sum) {
   const int64_t m = c->m, n = c->n;
   const int64_t ncon = (int64_t)c->h_con_idx.size() - 1;
@@ -241,24 +332,23 @@ int scale_pass(Ctx* c, int st, int phase, int use_sum) {
   double *tr = c->vtmp_m, *tc = c->vtmp_n;
   const bool hq = c->q_kind == HPR_Q_CSR;
 
-      row_stat_kernel<<<grid_for(n), 256, 0, c->stream>>>(n, c->AT.rowptr, c->AT.val, hq ? c->Q.rowptr : nullptr,
-                                                          hq ? c->Q.val : nullptr, use_sum, tc);
+      row_stat(c, n, c->AT.nnz + (hq ? c->Q.nnz : 0), c->AT.rowptr, c->AT.val, hq ? c->Q.rowptr : nullptr,
+               hq ? c->Q.val : nullptr, use_sum, tc);
       if (m > 0) {
-        row_stat_kernel<<<grid_for(m), 256, 0, c->stream>>>(m, c->A.rowptr, c->A.val, nullptr, nullptr, use_sum, tr);
-        if (ncon > 0)
-          block_kernel<<<grid_for(ncon), 256, 0, c->stream>>>(ncon, c->d_con_start, tr, st, phase, LOC_CON);
+        row_stat(c, m, c->A.nnz, c->A.rowptr, c->A.val, nullptr, nullptr, use_sum, tr);
+        if (ncon > 0) block_scale(c, ncon, m - c->m_lin, c->d_con_start, tr, st, phase, LOC_CON);
         HPR_TRY(vec_map(c, m, [=] __device__(int64_t i) { tr[i] = clamp4(tr[i]); }));
       }
-      if (nvar > 0) block_kernel<<<grid_for(nvar), 256, 0, c->stream>>>(nvar, c->d_var_start, tc, st, phase, LOC_VAR);
+      if (nvar > 0) block_scale(c, nvar, n - c->n_box, c->d_var_start, tc, st, phase, LOC_VAR);
       HPR_CUDA(c, cudaGetLastError());
       HPR_TRY(vec_map(c, n, [=] __device__(int64_t i) { tc[i] = clamp4(tc[i]); }));
       double *rn = c->row_norm, *cn = c->col_norm;
       HPR_TRY(vec_map(c, m, [=] __device__(int64_t i) { rn[i] *= tr[i]; }));
       HPR_TRY(vec_map(c, n, [=] __device__(int64_t i) { cn[i] *= tc[i]; }));
-      if (hq) scale_csr_kernel<<<grid_for(n), 256, 0, c->stream>>>(n, c->Q.rowptr, c->Q.col, c->Q.val, tc, tc);
+      if (hq) scale_csr(c, c->Q, tc, tc);
       if (m > 0) {
-        scale_csr_kernel<<<grid_for(m), 256, 0, c->stream>>>(m, c->A.rowptr, c->A.col, c->A.val, tr, tc);
-        scale_csr_kernel<<<grid_for(n), 256, 0, c->stream>>>(n, c->AT.rowptr, c->AT.col, c->AT.val, tc, tr);
+        scale_csr(c, c->A, tr, tc);
+        scale_csr(c, c->AT, tc, tr);
       }
       HPR_CUDA(c, cudaGetLastError());
       double *cc = c->c, *al = c->AL, *au = c->AU, *rh = c->soc_rhs, *rf = c->soc_rhs_full, *l = c->l, *u = c->u;
