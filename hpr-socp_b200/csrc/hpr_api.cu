@@ -124,16 +124,21 @@ void free_all(Ctx* c) {
 }
 
 bool is_finite(double x) { return std::isfinite(x); }
-bool not_nan(double x) { return !std::isnan(x); }
 bool finite_all(const double* v, int64_t n) { return host_all(v, n, is_finite); }
-bool nonan_all(const double* v, int64_t n) { return host_all(v, n, not_nan); }
 
-int put_vec(Ctx* c, double** d, const double* h, int64_t n) {
+// A device copy of a host array (zeros for a null array) that must pass
+// `check` (h2d_copy_checked); a failing value is reported with `what`
+// (HPR_E_BAD_INPUT)
+int put_checked(Ctx* c, double** d, const double* h, int64_t n, int check, const char* what) {
   HPR_TRY(dev_alloc_n(c, d, n));
-  if (n > 0) {
-    if (h) HPR_TRY(h2d_copy(c, *d, h, (size_t)n * sizeof(double)));
-    else HPR_CUDA(c, cudaMemsetAsync(*d, 0, n * sizeof(double), c->stream));
+  if (n <= 0) return HPR_OK;
+  if (!h) {
+    HPR_CUDA(c, cudaMemsetAsync(*d, 0, n * sizeof(double), c->stream));
+    return HPR_OK;
   }
+  bool ok = true;
+  HPR_TRY(h2d_copy_checked(c, *d, h, (size_t)n * sizeof(double), check, &ok));
+  if (!ok) return set_err(c, HPR_E_BAD_INPUT, what);
   return HPR_OK;
 }
 
@@ -823,11 +828,8 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   c->n_box = p->n_box;
   c->obj_constant = p->obj_constant;
   if (!std::isfinite(p->obj_constant)) return set_err(c, HPR_E_BAD_INPUT, "non-finite objective constant");
-  if (!finite_all(p->c, n)) return set_err(c, HPR_E_BAD_INPUT, "c has non-finite entries");
-  if (!nonan_all(p->l, n) || !nonan_all(p->u, n) || !nonan_all(p->AL, m) || !nonan_all(p->AU, m))
-    return set_err(c, HPR_E_BAD_INPUT, "NaN in bounds");
-  if (m - p->m_lin > 0 && p->soc_rhs && !finite_all(p->soc_rhs, m - p->m_lin))
-    return set_err(c, HPR_E_BAD_INPUT, "soc_rhs has non-finite entries");
+  // c, the bounds, soc_rhs and q_diag are checked as they are copied to the
+  // device (put_checked below)
   HPR_TRY(cone_index(c, p->soc_con_idx, p->n_soc_con_idx, base, p->m_lin, m, "soc_con_idx", c->h_con_idx));
   int64_t nbox = p->n_box;
   if (p->n_soc_var_idx > 1) {
@@ -857,12 +859,11 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
     }
   } else if (p->q_kind == HPR_Q_DIAG_LOWRANK) {
     if (!p->q_diag) return set_err(c, HPR_E_BAD_INPUT, "q_diag is null");
-    if (!finite_all(p->q_diag, n)) return set_err(c, HPR_E_BAD_INPUT, "q_diag has non-finite entries");
     int64_t k = p->F.nrows;
     vector<int32_t> frp, ftrp;
     HPR_TRY(upload_csr(c, p->F, base, k, n, "F", c->F, frp));
     HPR_TRY(transpose_csr(c, c->F, c->FT, ftrp));
-    HPR_TRY(put_vec(c, &c->qdiag, p->q_diag, n));
+    HPR_TRY(put_checked(c, &c->qdiag, p->q_diag, n, 1, "q_diag has non-finite entries"));
     c->has_q = true;
     qrp = ftrp;
     build_plan(frp, k, {}, c->planF);
@@ -901,18 +902,17 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   HPR_TRY(upload_plan(c, c->planY));
   if (c->has_q) HPR_TRY(upload_plan(c, c->planQ));
   // problem vectors
-  HPR_TRY(put_vec(c, &c->c, p->c, n));
-  HPR_TRY(put_vec(c, &c->l, p->l, n));
-  HPR_TRY(put_vec(c, &c->u, p->u, n));
-  HPR_TRY(put_vec(c, &c->AL, p->AL, m));
-  HPR_TRY(put_vec(c, &c->AU, p->AU, m));
-  HPR_TRY(put_vec(c, &c->soc_rhs, p->soc_rhs, m - p->m_lin));
-  {
-    vector<double> full(m, 0.0);
-    if (p->soc_rhs)
-      for (int64_t i = p->m_lin; i < m; ++i) full[i] = p->soc_rhs[i - p->m_lin];
-    HPR_TRY(put_vec(c, &c->soc_rhs_full, full.data(), m));
-  }
+  HPR_TRY(put_checked(c, &c->c, p->c, n, 1, "c has non-finite entries"));
+  HPR_TRY(put_checked(c, &c->l, p->l, n, 2, "NaN in bounds"));
+  HPR_TRY(put_checked(c, &c->u, p->u, n, 2, "NaN in bounds"));
+  HPR_TRY(put_checked(c, &c->AL, p->AL, m, 2, "NaN in bounds"));
+  HPR_TRY(put_checked(c, &c->AU, p->AU, m, 2, "NaN in bounds"));
+  HPR_TRY(put_checked(c, &c->soc_rhs, p->soc_rhs, m - p->m_lin, 1, "soc_rhs has non-finite entries"));
+  // soc_rhs aligned with the rows (zero on linear rows), assembled on the device
+  HPR_TRY(zero_vec(c, &c->soc_rhs_full, m));
+  if (m > p->m_lin)
+    HPR_CUDA(c, cudaMemcpyAsync(c->soc_rhs_full + p->m_lin, c->soc_rhs, (m - p->m_lin) * sizeof(double),
+                                cudaMemcpyDeviceToDevice, c->stream));
   // workspace (allocate_workspace, algorithm.jl:1443-1588)
   // length-n vectors (the variable side)
   double** nvecs[] = {&c->col_norm, &c->diag_Q, &c->fact1, &c->fact2, &c->fact,  &c->fact_M,

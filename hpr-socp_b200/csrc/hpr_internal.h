@@ -330,6 +330,9 @@ int transpose_csr(Ctx* c, const DevCSR& M, DevCSR& T, std::vector<int32_t>& trp)
 // stream: large arrays go through pinned chunks filled by several host
 // threads (the source may be reused as soon as this returns)
 int h2d_copy(Ctx* c, void* dst, const void* src, size_t bytes);
+// the same for an array of doubles, checked on the way (check 1: every
+// value finite, 2: no NaN); *ok is false if a value fails
+int h2d_copy_checked(Ctx* c, void* dst, const void* src, size_t bytes, int check, bool* ok);
 // device-to-host copy into a pageable host array after the work enqueued on
 // the context's stream; returns once the data is in dst
 int d2h_copy(Ctx* c, void* dst, const void* src, size_t bytes);

@@ -119,10 +119,11 @@ bool uses_pre_pock(int st) {
 
 // The three kernels below give each row (or cone) a group of G lanes that
 // walk its entries with stride G, so a warp's loads are coalesced and a long
-// row or cone is spread over G lanes instead of one thread.  G is chosen per
-// launch from the mean length (group_lanes).  Maxima do not depend on the
-// order; sums are added per lane and then over the group in a fixed shuffle
-// order, so the result depends on the data and G only.
+// row or cone is spread over G lanes instead of one thread (G = 1: one
+// thread per row, entries in order).  G is chosen per launch from the mean
+// length.  Maxima do not depend on the order; sums are added per lane and
+// then over the group in a fixed shuffle order, so the result depends on
+// the data and G only.
 template <int G>
 __device__ __forceinline__ double group_combine(double v, bool sum) {
 #pragma unroll
@@ -293,14 +294,14 @@ void row_stat_g(Ctx* c, int64_t nr, const int32_t* rp, const double* v, const in
                 int use_sum, double* out) {
   row_stat_kernel<G><<<grid_for(nr * G), 256, 0, c->stream>>>(nr, rp, v, qrp, qv, use_sum, out);
 }
+// Row statistics keep one thread per row (each thread's loads run ahead
+// along its row) unless rows are long on average; measured on B200 for the
+// benchmark's A and A' (means 17 and 12): 150 / 50 us per pass with one
+// thread per row against 388 / 300 us with 16 lanes per row.
 void row_stat(Ctx* c, int64_t nr, int64_t nnz, const int32_t* rp, const double* v, const int32_t* qrp,
               const double* qv, int use_sum, double* out) {
-  switch (group_lanes((double)nnz / (double)std::max<int64_t>(nr, 1))) {
-    case 4: row_stat_g<4>(c, nr, rp, v, qrp, qv, use_sum, out); break;
-    case 8: row_stat_g<8>(c, nr, rp, v, qrp, qv, use_sum, out); break;
-    case 16: row_stat_g<16>(c, nr, rp, v, qrp, qv, use_sum, out); break;
-    default: row_stat_g<32>(c, nr, rp, v, qrp, qv, use_sum, out); break;
-  }
+  if ((double)nnz / (double)std::max<int64_t>(nr, 1) <= 64.0) row_stat_g<1>(c, nr, rp, v, qrp, qv, use_sum, out);
+  else row_stat_g<32>(c, nr, rp, v, qrp, qv, use_sum, out);
 }
 void block_scale(Ctx* c, int64_t ncones, int64_t len, const int32_t* cs, double* t, int st, int ph, int loc) {
   const int g = group_lanes((double)len / (double)std::max<int64_t>(ncones, 1));
@@ -315,7 +316,9 @@ void block_scale(Ctx* c, int64_t ncones, int64_t len, const int32_t* cs, double*
 void scale_csr(Ctx* c, const DevCSR& M, const double* r, const double* cl) {
   const int64_t nr = M.nrows;
   if (nr == 0) return;
-  const int g = group_lanes((double)M.nnz / (double)nr);
+  // two to four entries per lane on average
+  const double mean = (double)M.nnz / (double)nr;
+  const int g = mean < 16.0 ? 4 : (mean < 32.0 ? 8 : (mean < 64.0 ? 16 : 32));
   const int grid = grid_for(nr * g);
   switch (g) {
     case 4: scale_csr_kernel<4><<<grid, 256, 0, c->stream>>>(nr, M.rowptr, M.col, M.val, r, cl); break;

@@ -184,20 +184,44 @@ bool stage_init(Stage& st, int device) {
 
 }  // namespace
 
-int h2d_copy(Ctx* c, void* dst, const void* src, size_t bytes) {
+namespace {
+
+// every double of v[0, n) passes (check 1: finite; check 2: not NaN); the
+// bit tests keep the loop branch-free
+bool doubles_ok(const void* p, size_t n, int check) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  uint64_t bad = 0;
+  for (size_t i = 0; i < n; ++i) {
+    uint64_t w;
+    std::memcpy(&w, b + 8 * i, 8);
+    const uint64_t a = w & 0x7fffffffffffffffull;
+    bad |= check == 1 ? (uint64_t)(a >= 0x7ff0000000000000ull) : (uint64_t)(a > 0x7ff0000000000000ull);
+  }
+  return bad == 0;
+}
+
+}  // namespace
+
+int h2d_copy(Ctx* c, void* dst, const void* src, size_t bytes) { return h2d_copy_checked(c, dst, src, bytes, 0, nullptr); }
+
+int h2d_copy_checked(Ctx* c, void* dst, const void* src, size_t bytes, int check, bool* ok) {
+  if (ok) *ok = true;
   if (bytes == 0) return HPR_OK;
   if (bytes < kStageMin || c->device < 0 || c->device >= kStageDevices) {
+    if (check && ok) *ok = doubles_ok(src, bytes / 8, check);
     HPR_CUDA(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
     return HPR_OK;
   }
   Stage& st = g_stage[c->device];
   std::lock_guard<std::mutex> lock(st.mu);
   if (!stage_init(st, c->device)) {
+    if (check && ok) *ok = doubles_ok(src, bytes / 8, check);
     HPR_CUDA(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
     return HPR_OK;
   }
   const size_t nchunks = (bytes + kStageChunk - 1) / kStageChunk;
   std::atomic<int> err{0};
+  std::atomic<bool> good{true};
   auto worker = [&](int t) {
     if (cudaSetDevice(c->device) != cudaSuccess) {
       err.store(1);
@@ -213,6 +237,8 @@ int h2d_copy(Ctx* c, void* dst, const void* src, size_t bytes) {
         return;
       }
       std::memcpy(st.buf[t][use], static_cast<const char*>(src) + off, len);
+      // the values are checked in the pinned chunk, while it is in cache
+      if (check && !doubles_ok(st.buf[t][use], len / 8, check)) good.store(false);
       if (cudaMemcpyAsync(static_cast<char*>(dst) + off, st.buf[t][use], len, cudaMemcpyHostToDevice, c->stream) !=
               cudaSuccess ||
           cudaEventRecord(st.ev[t][use], c->stream) != cudaSuccess) {
@@ -228,6 +254,7 @@ int h2d_copy(Ctx* c, void* dst, const void* src, size_t bytes) {
   worker(0);
   for (auto& x : th) x.join();
   if (err.load()) return set_err(c, HPR_E_CUDA, "staged host-to-device copy failed");
+  if (ok) *ok = good.load();
   return HPR_OK;
 }
 

@@ -6,6 +6,7 @@ The reference builds its GPU matrices from a validated SparseMatrixCSC
 variant of the same matrix must lead to bit-identical iterates.
 """
 import ctypes as C
+import functools
 
 import numpy as np
 import pytest
@@ -112,3 +113,33 @@ def test_malformed_matrix_is_rejected(defect, message):
         rp[-1] -= 1
     with pytest.raises(_abi.HPRError, match=message):
         Context(model, problem=_with_A(model, rp, ci, v))
+
+
+@functools.lru_cache(maxsize=None)
+def _vector_case(size):
+    return instances.config0(0) if size == "small" else instances.config1(1, scale=0.3)
+
+
+@pytest.mark.parametrize("field, value, message", [
+    ("c", np.inf, "c has non-finite entries"),
+    ("l", np.nan, "NaN in bounds"),
+    ("AU", np.nan, "NaN in bounds"),
+    ("soc_rhs", np.inf, "soc_rhs has non-finite entries"),
+])
+@pytest.mark.parametrize("size", ["small", "large"])
+def test_bad_problem_vector_is_rejected(field, value, message, size):
+    """c, the bounds and soc_rhs are checked while they are copied to the
+    device: a small array on the way to a plain copy, a large one (above the
+    4 MB staging threshold) chunk by chunk in the pinned staging buffers,
+    with the bad value in a late chunk.  Infinite bounds stay allowed."""
+    import dataclasses
+    model = _vector_case(size)
+    arr = np.array(getattr(model, field), dtype=np.float64)
+    arr[len(arr) - 3] = value
+    bad = dataclasses.replace(model, **{field: arr})
+    with pytest.raises(_abi.HPRError, match=message):
+        Context(bad)
+    if field == "l":
+        arr[len(arr) - 3] = -np.inf  # an infinite bound is not an error
+        with Context(dataclasses.replace(model, l=arr)):
+            pass
