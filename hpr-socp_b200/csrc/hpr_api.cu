@@ -837,19 +837,38 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   } else {
     c->h_var_idx.assign(1, n);
   }
-  // A and A' (validated, index-base converted and transposed on the device)
-  vector<int32_t> rp, trp;
+  // A and A' (validated, index-base converted and transposed on the device).
+  // Each side's tile plan is host work that needs only that side's row
+  // pointers, so it is built on a thread of its own while the device work,
+  // the other copies and the checks go on; the threads are joined before the
+  // plans are uploaded (and on every early return).
+  vector<int32_t> rp, trp, qrp;
+  vector<int64_t> vcones = c->h_var_idx.size() > 1 ? c->h_var_idx : vector<int64_t>();
+  vector<int64_t> ccones = c->h_con_idx.size() > 1 ? c->h_con_idx : vector<int64_t>();
+  int cap = 0;
+  struct Joiner {
+    std::vector<std::thread> t;
+    ~Joiner() {
+      for (auto& x : t)
+        if (x.joinable()) x.join();
+    }
+  } plans;
   HPR_TRY(upload_csr(c, p->A, base, m, n, "A", c->A, rp));
+  // problems below HPR_SMALL_PLAN_NNZ nonzeros get tiles of at most
+  // HPR_SMALL_TILE nonzeros: they occupy few warps, so shorter tiles shorten
+  // each launch's longest chain (0: every problem uses full tiles)
+  cap = c->A.nnz < (int64_t)HPR_SMALL_PLAN_NNZ ? (int)HPR_SMALL_TILE : 0;
+  plans.t.emplace_back([&] { build_plan(rp, m, ccones, c->planY, cap); });
   if (p->AT.rowptr) {
     HPR_TRY(upload_csr(c, p->AT, base, n, m, "AT", c->AT, trp));
     if (c->AT.nnz != c->A.nnz) return set_err(c, HPR_E_BAD_INPUT, "AT nnz differs from A");
   } else {
     HPR_TRY(transpose_csr(c, c->A, c->AT, trp));
   }
+  plans.t.emplace_back([&] { build_plan(trp, n, vcones, c->planX, cap); });
   // Q
   c->q_kind = p->q_kind;
   c->has_q = false;
-  vector<int32_t> qrp;
   if (p->q_kind == HPR_Q_CSR) {
     HPR_TRY(upload_csr(c, p->Q, base, n, n, "Q", c->Q, qrp));
     if (c->Q.nnz == 0) {
@@ -882,32 +901,19 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
                                 c->stream));
     HPR_CUDA(c, cudaStreamSynchronize(c->stream));
   }
-  // plans
-  vector<int64_t> vcones = c->h_var_idx.size() > 1 ? c->h_var_idx : vector<int64_t>();
-  vector<int64_t> ccones = c->h_con_idx.size() > 1 ? c->h_con_idx : vector<int64_t>();
-  // problems below HPR_SMALL_PLAN_NNZ nonzeros get tiles of at most
-  // HPR_SMALL_TILE nonzeros: they occupy few warps, so shorter tiles shorten
-  // each launch's longest chain (0: every problem uses full tiles)
-  const int cap = c->A.nnz < (int64_t)HPR_SMALL_PLAN_NNZ ? (int)HPR_SMALL_TILE : 0;
-  // the plans of A', A (and Q) are independent host work: built side by side
-  {
-    std::thread ty([&] { build_plan(rp, m, ccones, c->planY, cap); });
-    std::thread tq;
-    if (c->has_q) tq = std::thread([&] { build_plan(qrp, n, vcones, c->planQ, cap); });
-    build_plan(trp, n, vcones, c->planX, cap);
-    ty.join();
-    if (tq.joinable()) tq.join();
-  }
-  HPR_TRY(upload_plan(c, c->planX));
-  HPR_TRY(upload_plan(c, c->planY));
-  if (c->has_q) HPR_TRY(upload_plan(c, c->planQ));
-  // problem vectors
+  if (c->has_q) plans.t.emplace_back([&] { build_plan(qrp, n, vcones, c->planQ, cap); });
+  // problem vectors (while the plans are being built)
   HPR_TRY(put_checked(c, &c->c, p->c, n, 1, "c has non-finite entries"));
   HPR_TRY(put_checked(c, &c->l, p->l, n, 2, "NaN in bounds"));
   HPR_TRY(put_checked(c, &c->u, p->u, n, 2, "NaN in bounds"));
   HPR_TRY(put_checked(c, &c->AL, p->AL, m, 2, "NaN in bounds"));
   HPR_TRY(put_checked(c, &c->AU, p->AU, m, 2, "NaN in bounds"));
   HPR_TRY(put_checked(c, &c->soc_rhs, p->soc_rhs, m - p->m_lin, 1, "soc_rhs has non-finite entries"));
+  // plans
+  for (auto& x : plans.t) x.join();
+  HPR_TRY(upload_plan(c, c->planX));
+  HPR_TRY(upload_plan(c, c->planY));
+  if (c->has_q) HPR_TRY(upload_plan(c, c->planQ));
   // soc_rhs aligned with the rows (zero on linear rows), assembled on the device
   HPR_TRY(zero_vec(c, &c->soc_rhs_full, m));
   if (m > p->m_lin)
