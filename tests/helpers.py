@@ -106,3 +106,38 @@ def branch_disagreements(g, o, model):
     cy = np.sum(cone_branches(g.get("s"), g.get("y_bar"), model.SOC_con_idx) !=
                 cone_branches(o.get("s"), o.get("y_bar"), model.SOC_con_idx))
     return int(vx), int(cy)
+
+
+def edge_model(kind, seed=7):
+    """Degenerate shapes of the problem data, each a bounded problem with a
+    planted primal-dual point (instances._assemble):
+      lp_box     linear rows and boxed variables only, no cone anywhere;
+      one_cone   every variable in one cone of 300 (no boxed variable);
+      cones_only no linear row: every row of A in a constraint cone;
+      dim_one    cones of dimension 1 and 2 on both sides;
+      sparse     empty rows and empty columns in A;
+      no_rows    m = 0: boxes and cones only."""
+    from hprsocp_b200.instances import _assemble
+    rng = np.random.default_rng(seed)
+
+    def rnd(m, n, d):
+        return sp.random(m, n, density=d, random_state=rng, data_rvs=rng.standard_normal, format="csr")
+
+    if kind == "lp_box":
+        return _assemble(rng, rnd(150, 300, 0.03), sp.csr_matrix((0, 300)), 300, [], [])
+    if kind == "one_cone":
+        return _assemble(rng, rnd(100, 300, 0.03), rnd(100, 300, 0.03), 0, [300], [5] * 20)
+    if kind == "cones_only":
+        return _assemble(rng, sp.csr_matrix((0, 200)), rnd(120, 200, 0.04), 100, [10] * 10, [4] * 30)
+    if kind == "dim_one":
+        return _assemble(rng, rnd(60, 200, 0.04), rnd(30, 200, 0.04), 100, [1] * 50 + [2] * 25, [1] * 20 + [2] * 5)
+    if kind == "sparse":
+        A1 = rnd(120, 250, 0.02).tolil()
+        A1[10:20, :] = 0.0          # empty rows
+        A1[:, 200:230] = 0.0        # empty columns
+        A2 = rnd(40, 250, 0.02).tolil()
+        A2[:, 200:230] = 0.0
+        return _assemble(rng, A1.tocsr(), A2.tocsr(), 150, [10] * 10, [4] * 10)
+    if kind == "no_rows":
+        return _assemble(rng, sp.csr_matrix((0, 200)), sp.csr_matrix((0, 200)), 100, [10] * 10, [])
+    raise ValueError(kind)
