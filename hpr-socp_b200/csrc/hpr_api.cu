@@ -14,6 +14,9 @@
 #ifndef HPR_SMALL_PLAN_NNZ
 #define HPR_SMALL_PLAN_NNZ 0
 #endif
+#ifndef HPR_MID_TILE
+#define HPR_MID_TILE 704  // nonzeros per tile of a mid-size matrix (below)
+#endif
 #ifndef HPR_SMALL_TILE
 #define HPR_SMALL_TILE 256
 #endif
@@ -858,6 +861,18 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
   // HPR_SMALL_TILE nonzeros: they occupy few warps, so shorter tiles shorten
   // each launch's longest chain (0: every problem uses full tiles)
   cap = c->A.nnz < (int64_t)HPR_SMALL_PLAN_NNZ ? (int)HPR_SMALL_TILE : 0;
+  // A mid-size matrix (a million nonzeros or more, but fewer than two full
+  // tiles per resident warp) gets HPR_MID_TILE-nonzero tiles: its launches
+  // are bound by each warp's chain of tile steps rather than by the bytes.
+  // Measured on B200 on the 4.4M-nonzero Q-path instance (about 1.2 full
+  // tiles per warp), iterations/s with tiles of 320 / 416 / 640 / 704 /
+  // 1024 nonzeros: 6388 / 6482 / 6717 / 6781 / 6455 (means of six runs, one box).
+  if (cap == 0 && c->A.nnz >= ((int64_t)1 << 20) && HPR_MID_TILE < kNnzTile) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    const int64_t warps = (int64_t)sms * HPR_ENGINE_MINB * kWarpsPerCta;
+    if (c->A.nnz < 2 * warps * (int64_t)kNnzTile) cap = HPR_MID_TILE;
+  }
   plans.t.emplace_back([&] { build_plan(rp, m, ccones, c->planY, cap); });
   if (p->AT.rowptr) {
     HPR_TRY(upload_csr(c, p->AT, base, n, m, "AT", c->AT, trp));

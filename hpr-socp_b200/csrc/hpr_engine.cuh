@@ -599,12 +599,12 @@ __device__ void process_warp_tile(const EngineArgs& a, Epi& epi, int tix, WarpSm
   // descriptor is read again afterwards (an L1 hit), which keeps registers
   // for nonzeros in flight
   const int nnz = tp->nze - tp->nzb;
-  const uint32_t desc = a.pv.desc[(int64_t)tix * 32 + lane];
+  const uint64_t desc = a.pv.desc[(int64_t)tix * 32 + lane];
   const int R = (nnz + 31) >> 5;
   int my = nnz - lane * R;
   my = my < 0 ? 0 : (my > R ? R : my);
   const uint64_t pol = HPR_ENGINE_STREAM == 2 ? l2_evict_first_policy() : 0;
-  const uint32_t heads = desc & ((1u << kDescOrdShift) - 1u);
+  const uint32_t heads = (uint32_t)desc;
   const int j0 = (int)(desc >> kDescOrdShift);
   Vals<Epi::kSlots> v0, v1;
   if (HPR_ENGINE_PREFETCH && tp->kind != TASK_LONG_PART) {

@@ -25,9 +25,13 @@ namespace hpr {
 //   kThreads is the block size of the plain reduction and map kernels.
 // ---------------------------------------------------------------------------
 constexpr int kThreads = 256;
-// 704 = 11 gather rounds of 64 (measured best on B200)
+// 1024 = 32 runs of 32 (the most a run's 32 row-start bits describe; with
+// at most 64 rows a tile rarely holds more).  Measured on B200, the
+// benchmark SOCP: 512 / 608 / 704 / 800 / 1024 nonzeros per tile give
+// 3340 / 3460 / 3551 / 3583 (same box) and 704 / 1024 give 3472 / 3632
+// (another box) iterations/s.
 #ifndef HPR_NNZ_TILE
-#define HPR_NNZ_TILE 704
+#define HPR_NNZ_TILE 1024
 #endif
 constexpr int kNnzTile = HPR_NNZ_TILE;
 #ifndef HPR_ENGINE_ROWCAP
@@ -61,9 +65,9 @@ static_assert(sizeof(Task) == 32, "Task layout");
 // L, and stored lane-interleaved: element k of run L sits at slot
 // sbase + 32 k + L of the plan's tiled column/value arrays, so each load of
 // the warp is coalesced while every lane adds its own run in column order.
-// `desc[32 t + L]` holds the row starts inside run L (bit k: a non-empty row
-// begins at run element k) and, from bit kDescOrdShift, the number of
-// non-empty rows that begin in runs 0..L-1.  `nonempty` marks the tile's
+// `desc[32 t + L]` holds the row starts inside run L in its low 32 bits (bit
+// k: a non-empty row begins at run element k) and, from bit kDescOrdShift,
+// the number of non-empty rows that begin in runs 0..L-1.  `nonempty` marks the tile's
 // non-empty rows (bit r for row rb + r).
 struct TileRun {
   uint64_t nonempty;
@@ -71,7 +75,7 @@ struct TileRun {
   int32_t pad;
 };
 static_assert(sizeof(TileRun) == 16, "TileRun layout");
-constexpr int kDescOrdShift = 25;
+constexpr int kDescOrdShift = 32;
 static_assert(kNnzTile <= 32 * kDescOrdShift, "a run's row-start bits must fit below kDescOrdShift");
 
 // A cone of more than kSmallConeMax rows (or nonzeros beyond one tile) is
@@ -97,7 +101,7 @@ struct Plan {
   int32_t npartials = 0;  // long-row partial sums
   int32_t ncparts = 0;    // big-cone slices (norm shares)
   std::vector<TileRun> runs;   // per tile (run layout)
-  std::vector<uint32_t> desc;  // per tile and lane (run layout)
+  std::vector<uint64_t> desc;  // per tile and lane (run layout)
   int64_t tslots = 0;          // slots of the tiled arrays (nonzeros + run padding)
   // device copies
   Task* d_tasks = nullptr;
@@ -109,7 +113,7 @@ struct Plan {
   double* d_raw = nullptr;       // big-cone raw values (nrows)
   int32_t* d_ctr = nullptr;      // [0] tile counter, [1] finished warps (CTAs in the static form)
   TileRun* d_runs = nullptr;
-  uint32_t* d_desc = nullptr;
+  uint64_t* d_desc = nullptr;
   double* d_cpart = nullptr;      // big-cone norm shares per slice
   double* d_bignorm = nullptr;    // published norm per big cone
   int32_t* d_big_ready = nullptr; // 1 once the norm is published (reset by the last apply tile)
@@ -179,7 +183,7 @@ struct PlanView {
   int32_t ntasks, nbig, nlng;
   // run layout
   const TileRun* runs;
-  const uint32_t* desc;
+  const uint64_t* desc;
   const int32_t* tcol;
   const double* tval;
   const float* tval32;

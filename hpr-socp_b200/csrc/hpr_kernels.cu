@@ -49,7 +49,7 @@ int upload_plan(Ctx* c, Plan& p) {
   HPR_CUDA(c, cudaMemsetAsync(p.d_apply_cnt, 0, std::max<int64_t>(1, nb) * sizeof(int32_t), c->stream));
   if (nt) {
     HPR_CUDA(c, cudaMemcpyAsync(p.d_runs, p.runs.data(), nt * sizeof(TileRun), cudaMemcpyHostToDevice, c->stream));
-    HPR_CUDA(c, cudaMemcpyAsync(p.d_desc, p.desc.data(), nt * 32 * sizeof(uint32_t), cudaMemcpyHostToDevice,
+    HPR_CUDA(c, cudaMemcpyAsync(p.d_desc, p.desc.data(), nt * 32 * sizeof(uint64_t), cudaMemcpyHostToDevice,
                                 c->stream));
   }
   if (nt)

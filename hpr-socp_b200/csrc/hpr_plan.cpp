@@ -239,7 +239,7 @@ void build_runs(const std::vector<int32_t>& rp, Plan& plan) {
     }
     uint32_t before = 0;
     for (int L = 0; L < 32; ++L) {
-      plan.desc[ti * 32 + L] = heads[L] | (before << kDescOrdShift);
+      plan.desc[ti * 32 + L] = (uint64_t)heads[L] | ((uint64_t)before << kDescOrdShift);
       before += (uint32_t)__builtin_popcount(heads[L]);
     }
   }
