@@ -7,6 +7,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <thread>
 
 #include "hpr_engine.cuh"
@@ -706,6 +707,42 @@ int vec_ptr(Ctx* c, int which, double** p, int64_t* len) {
 }
 }  // namespace
 
+namespace hpr {
+namespace {
+// A context's small pinned host buffers (the reduction read-back lanes and
+// the state copy) are 1 KB slots of process-wide pinned slabs: a
+// cudaMallocHost / cudaFreeHost pair per context costs milliseconds
+// (cudaFreeHost measured 1-10 ms when a benchmark context is destroyed).
+// The slabs live until the process exits.
+constexpr size_t kPinSlot = 1024;
+constexpr int kPinSlotsPerSlab = 256;
+std::mutex g_pin_mu;
+std::vector<void*> g_pin_free;
+
+void* pin_get() {
+  std::lock_guard<std::mutex> lock(g_pin_mu);
+  if (g_pin_free.empty()) {
+    char* slab = nullptr;
+    if (cudaHostAlloc((void**)&slab, kPinSlot * kPinSlotsPerSlab, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    for (int i = kPinSlotsPerSlab - 1; i >= 0; --i) g_pin_free.push_back(slab + (size_t)i * kPinSlot);
+  }
+  void* p = g_pin_free.back();
+  g_pin_free.pop_back();
+  return p;
+}
+
+void pin_put(void* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lock(g_pin_mu);
+  g_pin_free.push_back(p);
+}
+static_assert(64 * sizeof(double) <= kPinSlot && sizeof(DevState) <= kPinSlot, "pinned slot size");
+}  // namespace
+}  // namespace hpr
+
 extern "C" {
 
 int hpr_version(void) { return 10000; }
@@ -783,8 +820,8 @@ int hpr_create(int device, size_t budget, hpr_ctx** out) {
   c->budget = budget ? budget : (size_t)(0.9 * (double)fr);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaMallocHost(&c->h_red_out, 64 * sizeof(double)) != cudaSuccess ||
-      cudaMallocHost(&c->h_state, sizeof(DevState)) != cudaSuccess) {
+      !(c->h_red_out = static_cast<double*>(pin_get())) || !(c->h_state = static_cast<DevState*>(pin_get()))) {
+    pin_put(c->h_red_out);
     delete h;
     return HPR_E_CUDA;
   }
@@ -798,8 +835,8 @@ int hpr_destroy(hpr_ctx* h) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_all(c);
-  if (c->h_red_out) cudaFreeHost(c->h_red_out);
-  if (c->h_state) cudaFreeHost(c->h_state);
+  pin_put(c->h_red_out);
+  pin_put(c->h_state);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev_mid) cudaEventDestroy(c->ev_mid);
