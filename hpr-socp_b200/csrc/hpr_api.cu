@@ -910,14 +910,14 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
     const int64_t warps = (int64_t)sms * HPR_ENGINE_MINB * kWarpsPerCta;
     if (c->A.nnz < 2 * warps * (int64_t)kNnzTile) cap = HPR_MID_TILE;
   }
-  plans.t.emplace_back([&] { build_plan(rp, m, ccones, c->planY, cap); });
+  spawn_or_run(plans.t, [&] { build_plan(rp, m, ccones, c->planY, cap); });
   if (p->AT.rowptr) {
     HPR_TRY(upload_csr(c, p->AT, base, n, m, "AT", c->AT, trp));
     if (c->AT.nnz != c->A.nnz) return set_err(c, HPR_E_BAD_INPUT, "AT nnz differs from A");
   } else {
     HPR_TRY(transpose_csr(c, c->A, c->AT, trp));
   }
-  plans.t.emplace_back([&] { build_plan(trp, n, vcones, c->planX, cap); });
+  spawn_or_run(plans.t, [&] { build_plan(trp, n, vcones, c->planX, cap); });
   // Q
   c->q_kind = p->q_kind;
   c->has_q = false;
@@ -953,7 +953,7 @@ int hpr_upload(hpr_ctx* h, const hpr_problem* p) {
                                 c->stream));
     HPR_CUDA(c, cudaStreamSynchronize(c->stream));
   }
-  if (c->has_q) plans.t.emplace_back([&] { build_plan(qrp, n, vcones, c->planQ, cap); });
+  if (c->has_q) spawn_or_run(plans.t, [&] { build_plan(qrp, n, vcones, c->planQ, cap); });
   // problem vectors (while the plans are being built)
   HPR_TRY(put_checked(c, &c->c, p->c, n, 1, "c has non-finite entries"));
   HPR_TRY(put_checked(c, &c->l, p->l, n, 2, "NaN in bounds"));

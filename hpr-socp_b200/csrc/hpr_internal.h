@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <type_traits>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -342,6 +343,16 @@ int h2d_copy_checked(Ctx* c, void* dst, const void* src, size_t bytes, int check
 int d2h_copy(Ctx* c, void* dst, const void* src, size_t bytes);
 // pred(v[i]) for every i, checked on several host threads for long arrays
 bool host_all(const double* v, int64_t n, bool (*pred)(double));
+// Runs f on a new thread added to `pool`, or on the calling thread when no
+// thread can be started, so that no exception leaves the library.
+template <class F>
+void spawn_or_run(std::vector<std::thread>& pool, F f) {
+  try {
+    pool.emplace_back(f);
+  } catch (...) {
+    f();
+  }
+}
 // scaling (hpr_scale.cu)
 int run_scaling(Ctx* c, const hpr_params* p, hpr_scale_info* out);
 

@@ -250,7 +250,7 @@ int h2d_copy_checked(Ctx* c, void* dst, const void* src, size_t bytes, int check
   };
   const int nt = (int)std::min<size_t>(kStageThreads, nchunks);
   std::vector<std::thread> th;
-  for (int t = 1; t < nt; ++t) th.emplace_back(worker, t);
+  for (int t = 1; t < nt; ++t) spawn_or_run(th, [&worker, t] { worker(t); });
   worker(0);
   for (auto& x : th) x.join();
   if (err.load()) return set_err(c, HPR_E_CUDA, "staged host-to-device copy failed");
@@ -302,7 +302,7 @@ int d2h_copy(Ctx* c, void* dst, const void* src, size_t bytes) {
   };
   const int nt = (int)std::min<size_t>(kStageThreads, nchunks);
   std::vector<std::thread> th;
-  for (int t = 1; t < nt; ++t) th.emplace_back(worker, t);
+  for (int t = 1; t < nt; ++t) spawn_or_run(th, [&worker, t] { worker(t); });
   worker(0);
   for (auto& x : th) x.join();
   if (err.load()) return set_err(c, HPR_E_CUDA, "staged device-to-host copy failed");
@@ -327,7 +327,7 @@ bool host_all(const double* v, int64_t n, bool (*pred)(double)) {
       }
   };
   std::vector<std::thread> th;
-  for (int t = 1; t < nt; ++t) th.emplace_back(part, t);
+  for (int t = 1; t < nt; ++t) spawn_or_run(th, [&part, t] { part(t); });
   part(0);
   for (auto& x : th) x.join();
   return good.load();
